@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Benchmark of the pbpic B200 step: particle-steps/s on one B200, FP32 mixed
+vs FP64 plain, at a stated energy error.
+
+Workload: the GEM Harris sheet on 1024x512 cells with 100 particles per cell
+per species (104,857,600 particles), conducting walls in y, seeded synthetic
+loading. A step is push + field solve + counting sort (sort every step).
+Timing: device time with CUDA events on the library's stream, warm-up steps
+untimed, max over ranks. The particle state (2.5 GB mixed, 4.6 GB plain) is
+far larger than L2, so no flush is needed between steps.
+
+--impl reference times the CPU restatement of the reference (oracle/, OpenMP
+over all host threads) on a bounded sample of the same workload.
+Multi-GPU: independent replicas per rank (the single-domain step does not
+shard here), weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy error"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="harris_1024x512_ppc100")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--sort-every", type=int, default=1)
+    return ap.parse_args()
+
+
+def workload(name, seed_offset=0):
+    from pbpic_b200 import configs
+    cfg, ld = configs.WORKLOADS[name]()
+    ld = dict(ld, seed=ld["seed"] + seed_offset)
+    return cfg, ld
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.lines = []
+        self.active = False
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            if self.active:
+                self.lines.append(line.strip())
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------- GPU
+def run_gpu(args, rank, world, dist):
+    import torch
+
+    import pbpic_b200
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    cfg, ld = workload(args.workload, seed_offset=rank)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    sampler = ClockSampler(dev)
+    for prec in (["fp32"] if args.no_fp64 else ["fp32", "fp64"]):
+        n = pbpic_b200.Simulation(**cfg, precision=prec, capacity=1).loader_count(**ld)
+        with pbpic_b200.Simulation(**cfg, precision=prec, capacity=n) as s:
+            s.set_stream(stream.cuda_stream)
+            s.init_plasma(**ld)
+            s.step(args.warmup, sort_every=args.sort_every)
+            s.synchronize()
+            barrier()
+            torch.cuda.synchronize()
+            K = args.steps
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+            launches0 = pbpic_b200.kernel_launches()
+            if prec == "fp32":
+                sampler.active = True
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            for k in range(K):
+                ev[k][0].record(stream)
+                s.pusher()
+                ev[k][1].record(stream)
+                s.fieldsolver()
+                ev[k][2].record(stream)
+                if args.sort_every > 0 and s.itime() % args.sort_every == 0:
+                    s.countingsort()
+                ev[k][3].record(stream)
+            end.record(stream)
+            torch.cuda.synchronize()
+            sampler.active = False
+            launches = pbpic_b200.kernel_launches() - launches0
+            barrier()
+            total_ms = max_over_ranks(start.elapsed_time(end))
+            t_push = np.mean([e[0].elapsed_time(e[1]) for e in ev])
+            t_field = np.mean([e[1].elapsed_time(e[2]) for e in ev])
+            t_sort = np.mean([e[2].elapsed_time(e[3]) for e in ev])
+            hist = s.energy_history()
+            tot = hist.sum(axis=1)
+            results[prec] = dict(n=n, total_ms=total_ms, ms_per_step=total_ms / K, t_push=t_push, t_field=t_field,
+                                 t_sort=t_sort, launches=launches, hist=hist,
+                                 energy_drift=float(abs(tot[-1] / tot[0] - 1.0)),
+                                 gauss=s.gauss_residual(), flux=s.reconnected_flux(), status=s.status())
+    clocks = sampler.stop()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, cfg, ld, stream, barrier, max_over_ranks)
+    return cfg, results, clocks, e2e
+
+
+def run_e2e(args, cfg, ld, stream, barrier, max_over_ranks):
+    """The same step through the C ABI with host-resident reference records:
+    H2D of the initial particles (pinned), K steps each followed by a D2H read
+    of the energies (totene row), and a D2H store of the final particles."""
+    import torch
+
+    import pbpic_b200
+    prec = "fp32"
+    n = pbpic_b200.Simulation(**cfg, precision=prec, capacity=1).loader_count(**ld)
+    host = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True).numpy().view(pbpic_b200.PARTICLE_F32)
+    out = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True).numpy().view(pbpic_b200.PARTICLE_F32)
+    K = args.steps
+    with pbpic_b200.Simulation(**cfg, precision=prec, capacity=n) as s:
+        s.set_stream(stream.cuda_stream)
+        s.init_plasma(**ld)
+        import ctypes
+        from pbpic_b200 import _lib as L
+        got = ctypes.c_int64()
+        L.check(L.lib().pbpic_store_particles_f32(s.handle, L.ptr(host), n, ctypes.byref(got)))
+        en = torch.empty(4, dtype=torch.float64, pin_memory=True).numpy()
+        s.step(args.warmup, sort_every=1)
+        s.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        L.check(L.lib().pbpic_load_particles_f32(s.handle, L.ptr(host), n))
+        s.countingsort()
+        for _ in range(K):
+            s.step(1, sort_every=args.sort_every)
+            L.check(L.lib().pbpic_energies(s.handle, L.ptr(en)))
+        L.check(L.lib().pbpic_store_particles_f32(s.handle, L.ptr(out), n, ctypes.byref(got)))
+        dt = time.perf_counter() - t0
+    dt = max_over_ranks(dt)
+    return dict(seconds=dt, n=n, K=K, h2d=n * 32 / K, d2h=32 + n * 32 / K)
+
+
+# ---------------------------------------------------------------------- CPU
+def run_cpu_sample(workload_name, steps, seed_offset=0):
+    """The oracle (OpenMP over all host threads) on a bounded sample of the
+    workload: the same grid and physics with 1/4 of the particles per cell."""
+    from oracle import oracle as O
+    from pbpic_b200 import configs
+    base = configs.WORKLOADS[workload_name]
+    cfg, ld = base()
+    ppc = max(1, ld["ppc"] // 4)
+    if workload_name.startswith("harris"):
+        cfg, ld = configs.harris(cfg["mx"], cfg["my"], ppc, ld["seed"] + seed_offset,
+                                 mime=cfg["mime"], nb=ld["nb"], bguide=ld["bguide"], dx=cfg["dx"])
+    else:
+        cfg, ld = base(mx=cfg["mx"], my=cfg["my"], ppc=ppc)
+    p, yee = O.load_plasma(cfg, ld)
+    o = O.Oracle(**cfg)
+    o.load_particles(p)
+    del p
+    o.set_fields(yee)
+    nth = O.max_threads()
+    o.omp_countingsort(nth)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.omp_pusher(nth)
+        o.fieldsolver()
+        o.omp_countingsort(nth)
+    dt = time.perf_counter() - t0
+    n = o.L.orc_nptl(o.h)
+    o.close()
+    return dict(value=n * steps / dt, cores=nth, n=n, steps=steps, seconds=dt,
+                sample=f"{cfg['mx']}x{cfg['my']} cells, {ppc} particles/cell/species ({n} particles), {steps} steps "
+                       "of push+fieldsolve+sort, FP64, OpenMP over all host threads")
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = max(1, min(args.steps, 2))
+        for _ in range(max(0, min(args.warmup, 1))):
+            pass
+        r = run_cpu_sample(args.workload, steps)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": r["steps"], "warmup": 0, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: seeded Philox Harris sheet",
+                "config": {"workload": args.workload, "sample": r["sample"]},
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    cfg, res, clocks, e2e = run_gpu(args, rank, world, dist)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_sample(args.workload, 4)
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    m = res["fp32"]
+    n = m["n"]
+    K = args.steps
+    value = world * n * K / (m["total_ms"] * 1e-3)
+    peak, peak_kind = measured_peak_hbm()
+    bytes_push = 48.0 * n  # read + write of cell (4 B), offsets (2x4 B), momenta (3x4 B)
+    achieved_push = bytes_push / (m["t_push"] * 1e-3) / 1e9
+    cells = cfg["mx"] * cfg["my"]
+    step_bytes = 48.0 * n + (48.0 * n if args.sort_every == 1 else 48.0 * n / max(args.sort_every, 1)) + 60.0 * cells
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (int64 fixed-point current, f64 energies)", "data": "synthetic: seeded Philox GEM Harris sheet",
+        "config": {"workload": args.workload, "grid": f"{cfg['mx']}x{cfg['my']}", "particles": n,
+                   "step": "push+fieldsolve+sort", "sort_every": args.sort_every, "ybc": "conducting",
+                   "l2": "inputs larger than L2 (particle state 2.5 GB)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved_push, "peak": peak, "unit": "GB/s",
+                     "frac": achieved_push / peak, "traffic": None, "kernel": "k_push<float,true>",
+                     "bytes_per_launch": bytes_push, "peak_kind": peak_kind,
+                     "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak},
+        "phase_ms": {"push": m["t_push"], "fieldsolve": m["t_field"], "sort": m["t_sort"]},
+        "energy": {"mixed_drift": m["energy_drift"], "gauss_residual": m["gauss"], "reconnected_flux": m["flux"]},
+        "gpu_launches": m["launches"],
+        "clocks": clocks,
+    }
+    if "fp64" in res:
+        d = res["fp64"]
+        vd = world * d["n"] * K / (d["total_ms"] * 1e-3)
+        hm, hd = m["hist"], d["hist"]
+        rows = min(len(hm), len(hd))
+        rel = np.abs(hm[:rows].sum(1) - hd[:rows].sum(1)) / np.abs(hd[:rows].sum(1))
+        line["fp64_plain"] = {"value": vd, "ms_per_step": d["ms_per_step"],
+                              "phase_ms": {"push": d["t_push"], "fieldsolve": d["t_field"], "sort": d["t_sort"]},
+                              "push_gbs": 88.0 * d["n"] / (d["t_push"] * 1e-3) / 1e9,
+                              "energy_drift": d["energy_drift"], "gauss_residual": d["gauss"]}
+        line["mixed_over_fp64"] = value / vd
+        line["energy"]["mixed_vs_fp64_total_energy_rel_err_max"] = float(rel.max())
+    if e2e:
+        line["e2e"] = {"value": world * e2e["n"] * e2e["K"] / e2e["seconds"], "unit": UNIT,
+                       "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                       "what": "H2D of the initial reference particle records (pinned), K steps each with a D2H "
+                               "of the energies, D2H of the final particles"}
+    if cpu:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
+                                "sample": cpu["sample"]}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

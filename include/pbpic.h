@@ -1,0 +1,205 @@
+/*
+ * pbpic.h -- C ABI of the B200 implementation of pbpic's 2-D electromagnetic
+ * particle-in-cell time step (xiaocanli/pbpic, src/programs/pic2d.f90).
+ *
+ * The reference's step boundary is three argument-less Fortran subroutines
+ * acting on module globals of `module parameters` (pic2d.f90:4-142):
+ *     call pusher        (pic2d.f90:177, body 912-1217)
+ *     call fieldsolver   (pic2d.f90:178, body 678-860)
+ *     call countingsort  (pic2d.f90:161, 181, body 1303-1329)
+ * Here the globals become a handle that owns the device state, and each
+ * subroutine becomes one call. Every function returns 0 on success or a
+ * negative PBPIC_E* code; pbpic_last_error() describes the last failure of the
+ * calling thread. Calls are stream-ordered on the handle's stream (default:
+ * the legacy default stream) and a handle must be used by one host thread at a
+ * time. No type in these signatures depends on CUDA or PyTorch.
+ *
+ * Units follow the reference: lengths in ion inertial lengths d_i, time in
+ * 1/Omega_ci, velocities in v_A, momenta u = gamma v / c, B in B0, E in v_A B0
+ * (pic2d.f90:15-43, 969-1006).
+ */
+#ifndef PBPIC_H
+#define PBPIC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- errors */
+#define PBPIC_OK 0
+#define PBPIC_EINVAL (-1)    /* bad argument or configuration */
+#define PBPIC_ECUDA (-2)     /* a CUDA call failed */
+#define PBPIC_ENOMEM (-3)    /* device allocation failed */
+#define PBPIC_ECAPACITY (-4) /* more particles than the handle's capacity */
+#define PBPIC_ESTATE (-5)    /* call not valid in the handle's current state */
+
+/* ------------------------------------------------------- configuration */
+#define PBPIC_BC_PERIODIC 0   /* y periodic: the reference on one MPI rank (pic2d.f90:294-304) */
+#define PBPIC_BC_CONDUCTING 1 /* y conducting walls: reflection + PEC (not in the reference) */
+
+#define PBPIC_FP64_PLAIN 0 /* FP64 throughout; the drop-in form */
+#define PBPIC_FP32_MIXED 1 /* FP32 push/deposit/FDTD, int64 fixed-point current, FP64 energies */
+
+/* Reproduce reference quirks bit for bit (default: corrected behaviour). */
+#define PBPIC_COMPAT_BORIS 1 /* rotate the pre-kick momentum (pic2d.f90:985-987) */
+#define PBPIC_COMPAT_FOLD 2  /* drop jy deposited in column mx+2 (fold commented, pic2d.f90:1156) */
+#define PBPIC_COMPAT_RHO 4   /* mirrored CIC weights for rho (pic2d.f90:1285-1295) */
+
+/* Device status bits reported by pbpic_status(). */
+#define PBPIC_STATUS_CELL_JUMP 1 /* a particle moved more than one cell in a step (pic2d.f90:1008-1023 assumes at most one) */
+#define PBPIC_STATUS_NAN 2       /* a momentum became NaN or infinite */
+#define PBPIC_STATUS_UNSORTED 4  /* a push met a particle outside its tile (informational) */
+
+typedef struct pbpic_config {
+  int32_t mx, my;      /* cells in x and y (nx, ny of pic2d.f90:12; one domain) */
+  double dx, dy;       /* cell size, d_i (pic2d.f90:15) */
+  double dt;           /* time step, 1/Omega_ci (pic2d.f90:42) */
+  double cva;          /* c / v_A (pic2d.f90:20) */
+  double mime;         /* m_i / m_e (pic2d.f90:19) */
+  double in0;          /* 1 / (macro-particles per cell at density n0) (pic2d.f90:31) */
+  int32_t ybc;         /* PBPIC_BC_* */
+  int32_t precision;   /* PBPIC_FP64_PLAIN or PBPIC_FP32_MIXED */
+  int32_t compat;      /* PBPIC_COMPAT_* bits */
+  int32_t track_pid;   /* nonzero: carry the reference's per-particle pid through the step */
+  int64_t capacity;    /* maximum number of particles (both species) */
+  int32_t tile_rows;   /* cells per push tile along y (0: default) */
+  int32_t reserved;
+} pbpic_config;
+
+/* The reference's `type particle` (pic2d.f90:47-50): 32 bytes. grid is the
+ * 1-based cell my*(ix-1)+iy (y fastest), dx, dy the offset from the cell
+ * centre in [-0.5, 0.5], q = +1 (ion) or -1 (electron). */
+typedef struct pbpic_particle_f32 {
+  float dx, dy, ux, uy, uz;
+  int32_t grid, q, pid;
+} pbpic_particle_f32;
+
+/* The same record with double-precision reals (56 bytes with padding). */
+typedef struct pbpic_particle_f64 {
+  double dx, dy, ux, uy, uz;
+  int32_t grid, q, pid, pad;
+} pbpic_particle_f64;
+
+/* Seeded plasma loader (the reference loads a double Harris sheet from
+ * /dev/urandom, pic2d.f90:357-578; these loaders are seeded Philox4x64-10). */
+#define PBPIC_LOAD_UNIFORM 0    /* uniform Maxwellian, ppc pairs in every cell, uniform Bz = b0z */
+#define PBPIC_LOAD_HARRIS 1     /* GEM Harris sheet along y with background, psi0 perturbation */
+#define PBPIC_LOAD_TWO_STREAM 2 /* counter-drifting electron beams along x */
+#define PBPIC_LOAD_WEIBEL 3     /* electrons with T_perp / T_par = anisotropy */
+
+typedef struct pbpic_loader {
+  int32_t kind;
+  int32_t ppc;          /* macro-particles per cell per species (average) */
+  double vthe, vthi;    /* thermal speeds / c (electron, ion) */
+  double vdrift_e;      /* electron drift / c: Harris along z, two-stream beams along +-x */
+  double vdrift_i;      /* ion drift / c (Harris, along z) */
+  double lambda;        /* Harris half-thickness, d_i */
+  double nb;            /* Harris background density / n0 */
+  double psi0;          /* GEM perturbation, B0 d_i */
+  double bguide;        /* Harris guide field Bz, B0 */
+  double b0z;           /* uniform Bz of the other loaders, B0 */
+  double anisotropy;    /* Weibel T_perp / T_par */
+  uint64_t seed;
+  int32_t immobile_ions; /* nonzero: load electrons only (a fixed neutralising ion background) */
+  int32_t reserved;
+} pbpic_loader;
+
+typedef struct pbpic_handle pbpic_handle;
+
+/* ------------------------------------------------------------ lifecycle */
+/* Replaces the allocation part of `init` (pic2d.f90:197-308). */
+int pbpic_create(const pbpic_config* cfg, pbpic_handle** out);
+int pbpic_destroy(pbpic_handle* h);
+const char* pbpic_last_error(void);
+/* Stream for all subsequent work of the handle (a cudaStream_t passed as void*). */
+int pbpic_set_stream(pbpic_handle* h, void* stream);
+int pbpic_get_config(const pbpic_handle* h, pbpic_config* out);
+
+/* ------------------------------------------------------------- loading */
+/* Seeded loading of particles and initial fields; replaces initparticles and
+ * initfields (pic2d.f90:357-648). Leaves the particles sorted by cell. */
+int pbpic_init_plasma(pbpic_handle* h, const pbpic_loader* ld);
+/* Number of particles a loader produces for this handle's grid. */
+int pbpic_loader_count(const pbpic_handle* h, const pbpic_loader* ld, int64_t* n);
+
+/* Particles in the reference's record (ptl, pic2d.f90:70). Host buffers. */
+int pbpic_load_particles_f32(pbpic_handle* h, const pbpic_particle_f32* p, int64_t n);
+int pbpic_load_particles_f64(pbpic_handle* h, const pbpic_particle_f64* p, int64_t n);
+int pbpic_store_particles_f32(pbpic_handle* h, pbpic_particle_f32* p, int64_t cap, int64_t* n);
+int pbpic_store_particles_f64(pbpic_handle* h, pbpic_particle_f64* p, int64_t cap, int64_t* n);
+/* Structure-of-arrays variants (host buffers); q[] holds +1 / -1; pid may be NULL. */
+int pbpic_load_particles_soa_f64(pbpic_handle* h, int64_t n, const int32_t* grid, const int32_t* q,
+                                 const double* dx, const double* dy, const double* ux,
+                                 const double* uy, const double* uz, const int32_t* pid);
+int pbpic_store_particles_soa_f64(pbpic_handle* h, int64_t cap, int64_t* n, int32_t* grid, int32_t* q,
+                                  double* dx, double* dy, double* ux, double* uy, double* uz,
+                                  int32_t* pid);
+int pbpic_num_particles(const pbpic_handle* h, int64_t* n);
+
+/* Primary Yee fields, host buffer of 6 planes (ex, ey, ez, bx, by, bz), each
+ * mx x (my+1) values with y fastest; entry (i, j) is the reference's
+ * emf(i+1, j+1) (pic2d.f90:71). Row my is used only for the node-row
+ * components (ex, bx) with conducting walls. Loading recomputes the node
+ * averages (emfgrid) and the field energy. */
+int pbpic_load_fields_f64(pbpic_handle* h, const double* yee6);
+int pbpic_store_fields_f64(pbpic_handle* h, double* yee6);
+/* emfgrid (pic2d.f90:72) nodes 1..mx+1 x 1..my+1: (mx+1) x (my+1) x 8 values,
+ * record (ex, ey, ez, 0, bx, by, bz, 0), y fastest. */
+int pbpic_store_emfgrid_f64(pbpic_handle* h, double* grid8);
+/* denjr (pic2d.f90:73) after normalisation by in0 and guard folding, 4 planes
+ * (jx, jy, jz, rho) of mx x (my+1), y fastest, as left by the last push. */
+int pbpic_store_denjr_f64(pbpic_handle* h, double* j4);
+
+/* ---------------------------------------------------------------- step */
+/* pusher (pic2d.f90:912-1217): zero the current, gather + Boris + move +
+ * charge-conserving deposit + x wrap + y wrap or wall reflection + J fold,
+ * kinetic energies into the history. */
+int pbpic_push(pbpic_handle* h);
+/* fieldsolver (pic2d.f90:678-860): B half step, E full step, B half step,
+ * node averages, field energies into the history. */
+int pbpic_fieldsolve(pbpic_handle* h);
+/* countingsort (pic2d.f90:1303-1329): stable sort of the particles by cell. */
+int pbpic_sort(pbpic_handle* h);
+/* The reference time loop body (pic2d.f90:171-188) nsteps times:
+ * push, fieldsolve, and a sort every sort_every steps (0: never). */
+int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every);
+/* Wait for the handle's stream. */
+int pbpic_synchronize(pbpic_handle* h);
+
+/* ---------------------------------------------------------- diagnostics */
+/* totene(1:4, itime) of the last completed step (pic2d.f90:122, 653-673,
+ * 1055-1062): electron KE, ion KE, electric and magnetic energy in m_e c^2. */
+int pbpic_energies(pbpic_handle* h, double out[4]);
+/* Energy history rows 0..n-1 (row 0 is the initial state), 4 doubles per row. */
+int pbpic_energy_history(pbpic_handle* h, double* out, int32_t max_rows, int32_t* n_rows);
+/* Steps completed since loading (itime of pic2d.f90:171). */
+int pbpic_time_step(const pbpic_handle* h, int32_t* itime);
+/* Per-cell particle counts from the last sort (ptlalloc before the scan,
+ * pic2d.f90:1310-1313), mx*my int32 in reference grid order. */
+int pbpic_cell_counts(pbpic_handle* h, int32_t* counts);
+/* Gauss's law residual max |div E / cva^2 - rho| over interior nodes, with rho
+ * the CIC charge density (units of n0 e) of the current particle positions. */
+int pbpic_gauss_residual(pbpic_handle* h, double* out);
+/* Reconnected flux: half the sum of |By| along the node row my/2 times dx. */
+int pbpic_reconnected_flux(pbpic_handle* h, double* out);
+/* Device status bits (PBPIC_STATUS_*) accumulated since the last call; clears them. */
+int pbpic_status(pbpic_handle* h, int32_t* bits);
+/* Number of CUDA kernels this library has launched in the process (all handles). */
+int pbpic_kernel_launches(int64_t* count);
+
+/* ----------------------------------------------- stateless counting sort */
+/* Stable counting sort of n cell keys in [0, ncells): perm[j] is the index of
+ * the j-th key in sorted order and counts[c] the number of keys in cell c
+ * (both device pointers). The same algorithm as pbpic_sort, exposed on raw
+ * device buffers; allocates its scratch with cudaMalloc on each call.
+ * stream is a cudaStream_t passed as void*. Replaces the ordering part of
+ * countingsort (pic2d.f90:1303-1329). */
+int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
+                             int32_t* perm_dev, int32_t* counts_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBPIC_H */

@@ -1,0 +1,91 @@
+"""Named workloads of the pbpic B200 step and their derived parameters.
+
+Units follow the reference (pic2d.f90:15-43, 969-1006): lengths in d_i, time
+in 1/Omega_ci, velocities in v_A with c = cva v_A, momenta u = gamma v / c.
+For a plasma with frequency ratio wpe/wce and mass ratio mi/me,
+c / v_A = (wpe/wce) sqrt(mi/me). The time step is set by a Courant number
+C = c dt sqrt(1/dx^2 + 1/dy^2).
+"""
+import math
+
+from . import _lib as L
+
+
+def dt_for_cfl(cva, dx, dy, cfl=0.5):
+    return cfl / (cva * math.sqrt(1.0 / dx ** 2 + 1.0 / dy ** 2))
+
+
+def harris_thermal(mime, cva, ti_te):
+    """Electron and ion thermal speeds (units of c) of a Harris sheet in
+    pressure balance n0 (Ti + Te) = B0^2 / (2 mu0)."""
+    te = 1.0 / (2.0 * (1.0 + ti_te))  # Te / (m_i v_A^2)
+    vthe = math.sqrt(mime * te) / cva
+    vthi = vthe * math.sqrt(ti_te / mime)
+    return vthe, vthi
+
+
+def harris_drifts(lam, cva, ti_te):
+    """Drift speeds (units of c) carrying the sheet current: Bx = B0 tanh(y/lambda)
+    needs J_z = -(1/lambda) sech^2 in units of n0 e v_A, split as U_i/T_i = -U_e/T_e."""
+    du = -1.0 / (lam * cva)  # U_i - U_e
+    return du * ti_te / (1.0 + ti_te), -du / (1.0 + ti_te)
+
+
+def harris_in0(mx, my, dx, dy, ppc, lam, nb):
+    """1 / (macro-particles per cell at the sheet peak density n0)."""
+    npairs = ppc * mx * my
+    lx, ly = mx * dx, my * dy
+    cells_equiv = lx * (2.0 * lam + nb * ly) / (dx * dy)
+    return cells_equiv / npairs
+
+
+def uniform_c1(seed=0, mx=128, my=128, ppc=32):
+    """Uniform periodic electron-proton plasma: 128x128 cells, dx = dy = 0.05 d_e,
+    CFL 0.5, 32 particles per cell per species, mi/me = 25, Ti = Te, electron
+    thermal speed 0.1 c, uniform Bz with wpe/wce = 2."""
+    mime, cva = 25.0, 2.0 * math.sqrt(25.0)
+    dx = dy = 0.05 / math.sqrt(mime)  # 0.05 d_e in d_i
+    cfg = dict(mx=mx, my=my, dx=dx, dy=dy, dt=dt_for_cfl(cva, dx, dy), cva=cva, mime=mime,
+               in0=1.0 / ppc, ybc=L.BC_PERIODIC)
+    vthe = 0.1
+    ld = dict(kind=L.LOAD_UNIFORM, ppc=ppc, vthe=vthe, vthi=vthe / math.sqrt(mime), b0z=1.0, seed=seed)
+    return cfg, ld
+
+
+def harris(mx, my, ppc, seed, mime=25.0, wpe_wce=2.0, lam=0.5, nb=0.2, ti_te=5.0, psi0=0.1,
+           bguide=0.0, dx=0.1, cfl=0.5):
+    cva = wpe_wce * math.sqrt(mime)
+    dy = dx
+    vthe, vthi = harris_thermal(mime, cva, ti_te)
+    udi, ude = harris_drifts(lam, cva, ti_te)
+    cfg = dict(mx=mx, my=my, dx=dx, dy=dy, dt=dt_for_cfl(cva, dx, dy, cfl), cva=cva, mime=mime,
+               in0=harris_in0(mx, my, dx, dy, ppc, lam, nb), ybc=L.BC_CONDUCTING)
+    ld = dict(kind=L.LOAD_HARRIS, ppc=ppc, vthe=vthe, vthi=vthi, vdrift_e=ude, vdrift_i=udi,
+              lambda_=lam, nb=nb, psi0=psi0, bguide=bguide, seed=seed)
+    return cfg, ld
+
+
+def harris_c2(seed=1, mx=1024, my=512, ppc=100):
+    """GEM Harris sheet, 1024x512 cells of 0.1 d_i, 100 particles per cell per
+    species (~105M), lambda = 0.5 d_i, nb = 0.2 n0, Ti/Te = 5, wpe/wce = 2,
+    psi0 = 0.1 B0 d_i, conducting walls in y, periodic in x."""
+    return harris(mx, my, ppc, seed)
+
+
+def harris_c4(seed=3):
+    """The differentiable-form Harris sheet: 256x128 cells, 64 per cell per species."""
+    return harris(256, 128, 64, seed)
+
+
+def harris_c5(seed=4):
+    """Large Harris sheet: 4096x2048 cells, 100 per cell per species (~1.68B),
+    mi/me = 100, nb = 0.1 n0, guide field 0.2 B0."""
+    return harris(4096, 2048, 100, seed, mime=100.0, nb=0.1, bguide=0.2, dx=0.05)
+
+
+WORKLOADS = {
+    "uniform_128x128_ppc32": uniform_c1,
+    "harris_1024x512_ppc100": harris_c2,
+    "harris_256x128_ppc64": harris_c4,
+    "harris_4096x2048_ppc100": harris_c5,
+}

@@ -1,0 +1,207 @@
+// Yee-grid field solver (fieldsolver, pic2d.f90:678-860) and field energy
+// (fieldsenergy, pic2d.f90:653-673).
+//
+// Storage: each of ex, ey, ez, bx, by, bz is one plane of mx x S values
+// (S = my + 1), x-major with y fastest; entry (i, j) is the reference's
+// emf(i+1, j+1). Locations in cell units (node (i, j) at (i, j)):
+//   ex, bx at (i+1/2, j)      ("node rows": j = 0..my-1, with walls 0..my)
+//   ey, by at (i, j+1/2)      ("half rows": j = 0..my-1)
+//   ez, bz at (i+1/2, j+1/2)  (half rows)
+// x is periodic. y is periodic (the reference's 1-rank ghost exchange,
+// pic2d.f90:701-835, is a wrap) or bounded by perfectly conducting walls on
+// node rows 0 and my: ex = 0 on the walls, and the ghost half rows are images
+// (ez, by odd; ey, bz even). The reference stores the curl terms in its
+// `fields` record; here they are recomputed from the fields, which gives the
+// same interior values (the stored terms are refreshed from the same fields
+// before every use).
+#pragma once
+#include "device_common.cuh"
+
+namespace pbd {
+
+template <class T>
+struct FieldParams {
+  int mx, my, S, ybc;
+  T *ex, *ey, *ez, *bx, *by, *bz;
+  T dth, cdt, idx, idy;  // dt/2, dt*cva^2 (pic2d.f90:43, 742)
+  const void* jacc;      // 4 planes of accumulators (double or int64)
+  double jscale[4];      // accumulator -> normalised current (in0, fixed-point scale)
+  T* ng;                 // node grid (mx+1) x (my+1) x 8
+  double* fe_part;       // per-block field energy partial sums [grid][2]
+};
+
+__device__ __forceinline__ int wrapx(int i, int mx) { return i < 0 ? i + mx : (i >= mx ? i - mx : i); }
+
+// Value of a half-row component at row j in [-1, my]: wrap, or wall image
+// with sign `odd_sign` (-1: odd image, +1: even image).
+template <class T>
+__device__ __forceinline__ T half_row(const T* f, int i, int j, int my, int S, int ybc, T odd_sign) {
+  if (ybc == 0) {
+    j = j < 0 ? j + my : (j >= my ? j - my : j);
+    return f[(long long)i * S + j];
+  }
+  if (j < 0) return odd_sign * f[(long long)i * S];
+  if (j >= my) return odd_sign * f[(long long)i * S + my - 1];
+  return f[(long long)i * S + j];
+}
+
+// Node-row component at row j in [0, my]: wrap (row my is row 0) or the wall row.
+template <class T>
+__device__ __forceinline__ T node_row(const T* f, int i, int j, int my, int S, int ybc) {
+  if (ybc == 0 && j >= my) j -= my;
+  return f[(long long)i * S + j];
+}
+
+// B half step, pic2d.f90:688-690 / 801-803, with the curl of E as in 790-793.
+template <class T>
+__global__ void k_bhalf(FieldParams<T> a) {
+  const int rows = a.ybc == 0 ? a.my : a.my + 1;
+  const long long n = (long long)a.mx * rows;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / rows), j = (int)(k - (long long)i * rows);
+    const long long o = (long long)i * a.S + j;
+    // bx (node row j): dez_dy = (ez(i,j) - ez(i,j-1)) * idy
+    {
+      const T ezj = half_row(a.ez, i, j, a.my, a.S, a.ybc, T(-1));
+      const T ezm = half_row(a.ez, i, j - 1, a.my, a.S, a.ybc, T(-1));
+      const T d = (ezj - ezm) * a.idy;
+      a.bx[o] = a.bx[o] - a.dth * d;
+    }
+    if (j < a.my) {
+      const int im = wrapx(i - 1, a.mx), ip = wrapx(i + 1, a.mx);
+      // by: dez_dx = (ez(i,j) - ez(i-1,j)) * idx
+      const T dezdx = (a.ez[o] - a.ez[(long long)im * a.S + j]) * a.idx;
+      a.by[o] = a.by[o] + a.dth * dezdx;
+      // bz: dex_dy = (ex(i,j+1) - ex(i,j)) * idy, dey_dx = (ey(i+1,j) - ey(i,j)) * idx
+      const T exn = node_row(a.ex, i, j + 1, a.my, a.S, a.ybc);
+      const T dexdy = (exn - a.ex[o]) * a.idy;
+      const T deydx = (a.ey[(long long)ip * a.S + j] - a.ey[o]) * a.idx;
+      a.bz[o] = a.bz[o] + a.dth * (dexdy - deydx);
+    }
+  }
+}
+
+template <class Acc>
+__device__ __forceinline__ double jval(const void* jacc, long long idx) {
+  return (double)reinterpret_cast<const Acc*>(jacc)[idx];
+}
+
+// E full step, pic2d.f90:742-744 with the curl of B as in 733-739.
+template <class T, class Acc>
+__global__ void k_efull(FieldParams<T> a) {
+  const int rows = a.ybc == 0 ? a.my : a.my + 1;
+  const long long n = (long long)a.mx * rows;
+  const long long plane = (long long)a.mx * a.S;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / rows), j = (int)(k - (long long)i * rows);
+    const long long o = (long long)i * a.S + j;
+    // ex (node row j): dbz_dy = (bz(i,j) - bz(i,j-1)) * idy
+    if (a.ybc == 1 && (j == 0 || j == a.my)) {
+      a.ex[o] = T(0);  // tangential E on a perfect conductor
+    } else {
+      const T bzj = half_row(a.bz, i, j, a.my, a.S, a.ybc, T(1));
+      const T bzm = half_row(a.bz, i, j - 1, a.my, a.S, a.ybc, T(1));
+      const T dbzdy = (bzj - bzm) * a.idy;
+      const T jx = (T)(jval<Acc>(a.jacc, o) * a.jscale[0]);
+      a.ex[o] = a.ex[o] + a.cdt * (dbzdy - jx);
+    }
+    if (j < a.my) {
+      const int im = wrapx(i - 1, a.mx), ip = wrapx(i + 1, a.mx);
+      // ey: dbz_dx = (bz(i,j) - bz(i-1,j)) * idx
+      const T dbzdx = (a.bz[o] - a.bz[(long long)im * a.S + j]) * a.idx;
+      const T jy = (T)(jval<Acc>(a.jacc, plane + o) * a.jscale[1]);
+      a.ey[o] = a.ey[o] - a.cdt * (dbzdx + jy);
+      // ez: dby_dx = (by(i+1,j) - by(i,j)) * idx, dbx_dy = (bx(i,j+1) - bx(i,j)) * idy
+      const T dbydx = (a.by[(long long)ip * a.S + j] - a.by[o]) * a.idx;
+      const T bxn = node_row(a.bx, i, j + 1, a.my, a.S, a.ybc);
+      const T dbxdy = (bxn - a.bx[o]) * a.idy;
+      const T jz = (T)(jval<Acc>(a.jacc, 2 * plane + o) * a.jscale[2]);
+      a.ez[o] = a.ez[o] + a.cdt * (dbydx - dbxdy - jz);
+    }
+  }
+}
+
+// Node averages (emfgrid, pic2d.f90:838-845) and the field energy sums
+// (pic2d.f90:659-670; with walls the two wall rows carry weight 1/2).
+template <class T>
+__global__ void k_nodes(FieldParams<T> a) {
+  __shared__ double red[32];
+  const int NX = a.mx + 1, NY = a.my + 1;
+  const long long n = (long long)NX * NY;
+  double se = 0.0, sb = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int ia = (int)(k / NY), b = (int)(k - (long long)ia * NY);
+    const int i = ia == a.mx ? 0 : ia;
+    const int im = wrapx(i - 1, a.mx);
+    const long long oi = (long long)i * a.S, om = (long long)im * a.S;
+    const int bn = (a.ybc == 0 && b == a.my) ? 0 : b;  // node row
+    const T ex = (a.ex[oi + bn] + a.ex[om + bn]) * T(0.5);
+    const T bx = (a.bx[oi + bn] + a.bx[om + bn]) * T(0.5);
+    const T ey = (half_row(a.ey, i, b, a.my, a.S, a.ybc, T(1)) +
+                  half_row(a.ey, i, b - 1, a.my, a.S, a.ybc, T(1))) * T(0.5);
+    const T by = (half_row(a.by, i, b, a.my, a.S, a.ybc, T(-1)) +
+                  half_row(a.by, i, b - 1, a.my, a.S, a.ybc, T(-1))) * T(0.5);
+    const T ez = (half_row(a.ez, i, b, a.my, a.S, a.ybc, T(-1)) +
+                  half_row(a.ez, im, b, a.my, a.S, a.ybc, T(-1)) +
+                  half_row(a.ez, i, b - 1, a.my, a.S, a.ybc, T(-1)) +
+                  half_row(a.ez, im, b - 1, a.my, a.S, a.ybc, T(-1))) * T(0.25);
+    const T bz = (half_row(a.bz, i, b, a.my, a.S, a.ybc, T(1)) +
+                  half_row(a.bz, im, b, a.my, a.S, a.ybc, T(1)) +
+                  half_row(a.bz, i, b - 1, a.my, a.S, a.ybc, T(1)) +
+                  half_row(a.bz, im, b - 1, a.my, a.S, a.ybc, T(1))) * T(0.25);
+    T* g = a.ng + k * 8;
+    g[0] = ex;
+    g[1] = ey;
+    g[2] = ez;
+    g[3] = T(0);
+    g[4] = bx;
+    g[5] = by;
+    g[6] = bz;
+    g[7] = T(0);
+    if (ia < a.mx && (a.ybc == 1 || b < a.my)) {
+      const double w = (a.ybc == 1 && (b == 0 || b == a.my)) ? 0.5 : 1.0;
+      const T e2 = ex * ex + ey * ey + ez * ez;
+      const T b2 = bx * bx + by * by + bz * bz;
+      se += w * (double)e2;
+      sb += w * (double)b2;
+    }
+  }
+  const double te = block_sum(se, red);
+  const double tb = block_sum(sb, red);
+  if (threadIdx.x == 0) {
+    a.fe_part[2 * blockIdx.x] = te;
+    a.fe_part[2 * blockIdx.x + 1] = tb;
+  }
+}
+
+// Sum the per-tile kinetic and per-block field partials in a fixed order and
+// write one row (electron KE, ion KE, E energy, B energy) of the history.
+// Either pointer may be null, in which case that half of the row is kept.
+__global__ void k_energy_row(const double* ke_part, int nke, const double* fe_part, int nfe,
+                             double fe_scale, double fb_scale, double* row) {
+  __shared__ double red[32];
+  double s[4] = {0, 0, 0, 0};
+  if (ke_part)
+    for (int i = threadIdx.x; i < nke; i += blockDim.x) {
+      s[0] += ke_part[2 * i];
+      s[1] += ke_part[2 * i + 1];
+    }
+  if (fe_part)
+    for (int i = threadIdx.x; i < nfe; i += blockDim.x) {
+      s[2] += fe_part[2 * i];
+      s[3] += fe_part[2 * i + 1];
+    }
+  for (int c = 0; c < 4; ++c) {
+    const double t = block_sum(s[c], red);
+    if (threadIdx.x == 0) {
+      if (c < 2 && ke_part) row[c] = t;
+      if (c == 2 && fe_part) row[2] = t * fe_scale;
+      if (c == 3 && fe_part) row[3] = t * fb_scale;
+    }
+  }
+}
+
+}  // namespace pbd

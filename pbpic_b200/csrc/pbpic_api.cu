@@ -1,0 +1,982 @@
+// C ABI of the pbpic B200 step (include/pbpic.h): device state, kernel
+// orchestration and host<->device transfers.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/pbpic.h"
+#include "device_common.cuh"
+#include "kernels_field.cuh"
+#include "kernels_misc.cuh"
+#include "kernels_push.cuh"
+#include "kernels_sort.cuh"
+#include "pic_common.h"
+#include "pic_fields_init.h"
+
+using namespace pbd;
+
+namespace {
+
+thread_local std::string g_err = "";
+std::atomic<long long> g_launches{0};  // kernels launched by this library (all handles)
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return fail(PBPIC_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKLAUNCH(what)                                                                    \
+  do {                                                                                    \
+    g_launches.fetch_add(1, std::memory_order_relaxed);                                   \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) return fail(PBPIC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TRY(...)                   \
+  do {                             \
+    int r_ = (__VA_ARGS__);        \
+    if (r_ != PBPIC_OK) return r_; \
+  } while (0)
+
+int grid_for(int64_t n, int block, int maxblocks = 148 * 16) {
+  int64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > maxblocks) g = maxblocks;
+  return (int)g;
+}
+
+// ------------------------------------------------------------------ scan
+// Exclusive scan of n int32 in place. scratch holds the chunk totals of every
+// level: scan_scratch_ints(n) entries.
+int64_t scan_scratch_ints(int64_t n) {
+  int64_t tot = 0;
+  while (true) {
+    int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    tot += nb + 1;
+    if (nb <= 1) break;
+    n = nb;
+  }
+  return tot;
+}
+
+int scan_excl(cudaStream_t s, int32_t* data, int64_t n, int32_t* scratch) {
+  if (n <= 0) return PBPIC_OK;
+  int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  k_scan_local<<<(unsigned)nb, SCAN_BT, 0, s>>>(data, n, scratch);
+  CKLAUNCH("k_scan_local");
+  if (nb > 1) {
+    TRY(scan_excl(s, scratch, nb, scratch + nb + 1));
+    k_scan_add<<<(unsigned)nb, 256, 0, s>>>(data, n, scratch);
+    CKLAUNCH("k_scan_add");
+  }
+  return PBPIC_OK;
+}
+
+// ------------------------------------------------------------ radix sort
+int radix_passes(int32_t ncells) {
+  int bits = 1;
+  while (bits < 31 && (1ll << bits) < (int64_t)ncells) ++bits;
+  return (bits + 7) / 8;
+}
+
+int64_t radix_hist_ints(int64_t n) { return 256 * ((n + RTILE - 1) / RTILE); }
+
+// Stable LSD radix sort of keys k0[0..n) (values: the indices). Buffers k0/k1
+// and v0/v1 ping-pong; returns the buffer holding the permutation.
+int radix_sort(cudaStream_t s, int64_t n, int32_t ncells, int32_t* k0, int32_t* k1, int32_t* v0,
+               int32_t* v1, int32_t* rhist, int32_t* scan_scratch, int32_t** perm) {
+  const int passes = radix_passes(ncells);
+  const int nblocks = (int)((n + RTILE - 1) / RTILE);
+  int32_t *kin = k0, *kout = k1, *vin = nullptr, *vout = v1;
+  int32_t* other_v = v0;
+  for (int p = 0; p < passes; ++p) {
+    k_radix_up<<<nblocks, RB, 0, s>>>(kin, n, 8 * p, rhist, nblocks);
+    CKLAUNCH("k_radix_up");
+    TRY(scan_excl(s, rhist, (int64_t)256 * nblocks, scan_scratch));
+    k_radix_down<<<nblocks, RB, 0, s>>>(kin, vin, n, 8 * p, rhist, nblocks, kout, vout);
+    CKLAUNCH("k_radix_down");
+    std::swap(kin, kout);
+    vin = vout;
+    vout = other_v;
+    other_v = vin;
+  }
+  *perm = vin;
+  return PBPIC_OK;
+}
+
+template <class T>
+struct DevT {
+  static constexpr bool mixed = sizeof(T) == 4;
+};
+
+}  // namespace
+
+// ===================================================================== handle
+struct pbpic_handle {
+  pbpic_config cfg;
+  bool mixed = false;
+  size_t tsz = 8;
+  cudaStream_t stream = 0;
+  int S = 0, ncells = 0, TY = 0, tpc = 0, ntiles = 0;
+  int64_t n = 0, cap = 0;
+  uint32_t* cell[2] = {nullptr, nullptr};
+  void* comp[2][5] = {{nullptr}};
+  int32_t* pid[2] = {nullptr, nullptr};
+  int cur = 0;
+  void* f[6] = {nullptr};
+  void* ng = nullptr;
+  void* jacc = nullptr;
+  int32_t *counts = nullptr, *off = nullptr, *tile_off = nullptr;
+  double *ke_part = nullptr, *fe_part = nullptr;
+  int nfe = 0, nke = 0;
+  double* hist = nullptr;
+  int hist_rows = 0;
+  int itime = 0;
+  int* status = nullptr;
+  int32_t *keys[2] = {nullptr, nullptr}, *vals[2] = {nullptr, nullptr};
+  int32_t* rhist = nullptr;
+  int32_t* scan_scratch = nullptr;
+  bool sorted = false;
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  double* rho = nullptr;
+  double* dscalar = nullptr;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+int dalloc(pbpic_handle* h, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(PBPIC_ENOMEM, std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+  }
+  h->allocs.push_back(*p);
+  return PBPIC_OK;
+}
+
+template <class P>
+int dalloc(pbpic_handle* h, P** p, size_t bytes) {
+  void* q = nullptr;
+  int r = dalloc(h, &q, bytes);
+  *p = (P*)q;
+  return r;
+}
+
+int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
+
+int ensure_staging(pbpic_handle* h, size_t bytes) {
+  if (h->staging_bytes >= bytes) return PBPIC_OK;
+  if (h->staging) {
+    cudaFree(h->staging);
+    h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), h->staging));
+    h->staging = nullptr;
+  }
+  TRY(dalloc(h, &h->staging, bytes));
+  h->staging_bytes = bytes;
+  return PBPIC_OK;
+}
+
+int ensure_hist(pbpic_handle* h, int rows) {
+  if (rows <= h->hist_rows) return PBPIC_OK;
+  int nr = std::max(rows, h->hist_rows * 2);
+  double* nh = nullptr;
+  TRY(dalloc(h, &nh, (size_t)nr * 4 * sizeof(double)));
+  CK(cudaMemsetAsync(nh, 0, (size_t)nr * 4 * sizeof(double), h->stream));
+  if (h->hist) {
+    CK(cudaMemcpyAsync(nh, h->hist, (size_t)h->hist_rows * 4 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(h->hist);
+    h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), (void*)h->hist));
+  }
+  h->hist = nh;
+  h->hist_rows = nr;
+  return PBPIC_OK;
+}
+
+template <class T>
+T* P(pbpic_handle* h, int buf, int c) {
+  return (T*)h->comp[buf][c];
+}
+
+// ------------------------------------------------------------- constants
+template <class T, bool MIXED>
+PushParams<T> push_params(pbpic_handle* h) {
+  const pbpic_config& c = h->cfg;
+  PushParams<T> p;
+  p.mx = c.mx;
+  p.my = c.my;
+  p.S = h->S;
+  p.ybc = c.ybc;
+  p.compat = c.compat;
+  p.tile_rows = h->TY;
+  p.tiles_per_col = h->tpc;
+  p.ntiles = h->ntiles;
+  p.tile_off = h->tile_off;
+  const int b = h->cur;
+  p.cell = h->cell[b];
+  p.dx = P<T>(h, b, 0);
+  p.dy = P<T>(h, b, 1);
+  p.ux = P<T>(h, b, 2);
+  p.uy = P<T>(h, b, 3);
+  p.uz = P<T>(h, b, 4);
+  p.ng = (const T*)h->ng;
+  p.jacc = h->jacc;
+  const T dt = (T)c.dt, mime = (T)c.mime, cva = (T)c.cva, dx = (T)c.dx, dy = (T)c.dy;
+  for (int s = 0; s < 2; ++s) {
+    const T q = s == 0 ? T(1) : T(-1);
+    const T ms = s == 0 ? mime : T(1);
+    p.c0[s] = q * dt * mime / ms / T(2);  // pic2d.f90:969
+    p.c1[s] = p.c0[s] / cva;              // pic2d.f90:970
+    p.ms[s] = ms;
+    p.q[s] = q;
+    p.qx[s] = MIXED ? q : q * dx / dt;  // pic2d.f90:1237-1238
+    p.qy[s] = MIXED ? q : q * dy / dt;
+  }
+  p.dtcva = dt * cva;  // pic2d.f90:1004
+  p.idx = T(1) / dx;   // pic2d.f90:16
+  p.idy = T(1) / dy;
+  p.cva = cva;
+  p.ke_part = h->ke_part;
+  p.status = h->status;
+  return p;
+}
+
+template <class T, bool MIXED>
+FieldParams<T> field_params(pbpic_handle* h) {
+  const pbpic_config& c = h->cfg;
+  FieldParams<T> a;
+  a.mx = c.mx;
+  a.my = c.my;
+  a.S = h->S;
+  a.ybc = c.ybc;
+  a.ex = (T*)h->f[0];
+  a.ey = (T*)h->f[1];
+  a.ez = (T*)h->f[2];
+  a.bx = (T*)h->f[3];
+  a.by = (T*)h->f[4];
+  a.bz = (T*)h->f[5];
+  const T dt = (T)c.dt, cva = (T)c.cva;
+  const T cva2 = cva * cva;  // pic2d.f90:21
+  a.dth = dt / T(2);         // pic2d.f90:43
+  a.cdt = dt * cva2;         // pic2d.f90:742
+  a.idx = T(1) / (T)c.dx;
+  a.idy = T(1) / (T)c.dy;
+  a.jacc = h->jacc;
+  if (MIXED) {
+    a.jscale[0] = c.in0 * (c.dx / c.dt) * FIX_INV;
+    a.jscale[1] = c.in0 * (c.dy / c.dt) * FIX_INV;
+    a.jscale[2] = c.in0 * c.cva * FIX_INV;
+    a.jscale[3] = c.in0 * FIX_INV;
+  } else {
+    for (int k = 0; k < 4; ++k) a.jscale[k] = c.in0;
+  }
+  a.ng = (T*)h->ng;
+  a.fe_part = h->fe_part;
+  return a;
+}
+
+double fe_scale(const pbpic_config& c) { return 0.5 * c.mime / (c.cva * c.cva * c.cva * c.cva * c.in0); }
+double fb_scale(const pbpic_config& c) { return 0.5 * c.mime / (c.cva * c.cva * c.in0); }
+
+// ------------------------------------------------------------ operations
+template <class T, bool MIXED>
+int nodes_and_field_energy(pbpic_handle* h, int row) {
+  TRY(ensure_hist(h, row + 1));
+  FieldParams<T> a = field_params<T, MIXED>(h);
+  k_nodes<T><<<h->nfe, 256, 0, h->stream>>>(a);
+  CKLAUNCH("k_nodes");
+  k_energy_row<<<1, 256, 0, h->stream>>>(nullptr, 0, h->fe_part, h->nfe, fe_scale(h->cfg), fb_scale(h->cfg),
+                                          h->hist + (size_t)row * 4);
+  CKLAUNCH("k_energy_row");
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int kinetic_row(pbpic_handle* h, int row) {
+  TRY(ensure_hist(h, row + 1));
+  const int b = h->cur;
+  k_kinetic<T, MIXED><<<h->nke, 256, 0, h->stream>>>(h->n, h->cell[b], P<T>(h, b, 2), P<T>(h, b, 3),
+                                                      P<T>(h, b, 4), (T)h->cfg.mime, h->ke_part);
+  CKLAUNCH("k_kinetic");
+  k_energy_row<<<1, 256, 0, h->stream>>>(h->ke_part, h->nke, nullptr, 0, 0, 0, h->hist + (size_t)row * 4);
+  CKLAUNCH("k_energy_row");
+  return PBPIC_OK;
+}
+
+int set_unsorted_tiles(pbpic_handle* h) {
+  k_tile_off_uniform<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, h->stream>>>(h->ntiles, h->n, h->tile_off);
+  CKLAUNCH("k_tile_off_uniform");
+  h->sorted = false;
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_sort(pbpic_handle* h) {
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  CK(cudaMemsetAsync(h->counts, 0, (size_t)(h->ncells + 1) * 4, s));
+  const int b = h->cur, o = 1 - b;
+  if (n > 0) {
+    k_cell_keys<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->cell[b], n, h->cfg.my, h->keys[0], h->counts);
+    CKLAUNCH("k_cell_keys");
+  }
+  CK(cudaMemcpyAsync(h->off, h->counts, (size_t)(h->ncells + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  TRY(scan_excl(s, h->off, h->ncells + 1, h->scan_scratch));
+  if (n > 0) {
+    int32_t* perm = nullptr;
+    TRY(radix_sort(s, n, h->ncells, h->keys[0], h->keys[1], h->vals[0], h->vals[1], h->rhist, h->scan_scratch,
+                   &perm));
+    k_gather<T><<<grid_for(n, 256), 256, 0, s>>>(perm, n, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
+                                                  P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], h->cell[o], P<T>(h, o, 0),
+                                                  P<T>(h, o, 1), P<T>(h, o, 2), P<T>(h, o, 3), P<T>(h, o, 4),
+                                                  h->pid[o]);
+    CKLAUNCH("k_gather");
+    h->cur = o;
+  }
+  k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, h->cfg.my,
+                                                                  (int32_t)n, h->tile_off);
+  CKLAUNCH("k_tile_off");
+  h->sorted = true;
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_push(pbpic_handle* h) {
+  cudaStream_t s = h->stream;
+  TRY(ensure_hist(h, h->itime + 2));
+  CK(cudaMemsetAsync(h->jacc, 0, (size_t)4 * plane_elems(h) * 8, s));
+  PushParams<T> p = push_params<T, MIXED>(h);
+  const size_t smem = (size_t)16 * (h->TY + 3) * 8;
+  k_push<T, MIXED><<<h->ntiles, NTHREADS, smem, s>>>(p);
+  CKLAUNCH("k_push");
+  k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
+  CKLAUNCH("k_energy_row");
+  h->sorted = false;
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_fieldsolve(pbpic_handle* h) {
+  cudaStream_t s = h->stream;
+  FieldParams<T> a = field_params<T, MIXED>(h);
+  const int rows = h->cfg.ybc == 0 ? h->cfg.my : h->cfg.my + 1;
+  const int g = grid_for((int64_t)h->cfg.mx * rows, 256);
+  k_bhalf<T><<<g, 256, 0, s>>>(a);
+  CKLAUNCH("k_bhalf");
+  if (MIXED) k_efull<T, long long><<<g, 256, 0, s>>>(a);
+  else k_efull<T, double><<<g, 256, 0, s>>>(a);
+  CKLAUNCH("k_efull");
+  k_bhalf<T><<<g, 256, 0, s>>>(a);
+  CKLAUNCH("k_bhalf");
+  TRY(nodes_and_field_energy<T, MIXED>(h, h->itime + 1));
+  h->itime += 1;
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_load_fields(pbpic_handle* h, const double* yee6) {
+  const int64_t pe = plane_elems(h);
+  std::vector<T> tmp((size_t)pe);
+  for (int c = 0; c < 6; ++c) {
+    for (int64_t k = 0; k < pe; ++k) tmp[k] = (T)yee6[(size_t)c * pe + k];
+    CK(cudaMemcpyAsync(h->f[c], tmp.data(), (size_t)pe * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return nodes_and_field_energy<T, MIXED>(h, h->itime);
+}
+
+template <class T, bool MIXED>
+int do_store_fields(pbpic_handle* h, double* yee6) {
+  const int64_t pe = plane_elems(h);
+  std::vector<T> tmp((size_t)pe);
+  for (int c = 0; c < 6; ++c) {
+    CK(cudaMemcpyAsync(tmp.data(), h->f[c], (size_t)pe * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t k = 0; k < pe; ++k) yee6[(size_t)c * pe + k] = (double)tmp[k];
+  }
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_store_grid(pbpic_handle* h, double* g8) {
+  const size_t ne = (size_t)(h->cfg.mx + 1) * (h->cfg.my + 1) * 8;
+  std::vector<T> tmp(ne);
+  CK(cudaMemcpyAsync(tmp.data(), h->ng, ne * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t k = 0; k < ne; ++k) g8[k] = (double)tmp[k];
+  return PBPIC_OK;
+}
+
+int do_store_denjr(pbpic_handle* h, double* j4) {
+  const int64_t pe = plane_elems(h);
+  std::vector<double> acc((size_t)(4 * pe));
+  CK(cudaMemcpyAsync(acc.data(), h->jacc, (size_t)(4 * pe) * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const pbpic_config& c = h->cfg;
+  double sc[4];
+  if (h->mixed) {
+    sc[0] = c.in0 * (c.dx / c.dt) * FIX_INV;
+    sc[1] = c.in0 * (c.dy / c.dt) * FIX_INV;
+    sc[2] = c.in0 * c.cva * FIX_INV;
+    sc[3] = c.in0 * FIX_INV;
+  } else {
+    for (int k = 0; k < 4; ++k) sc[k] = c.in0;
+  }
+  for (int comp = 0; comp < 4; ++comp)
+    for (int64_t k = 0; k < pe; ++k) {
+      const size_t i = (size_t)comp * pe + k;
+      double v;
+      if (h->mixed) {
+        long long q;
+        memcpy(&q, &acc[i], 8);
+        v = (double)q;
+      } else {
+        v = acc[i];
+      }
+      j4[i] = v * sc[comp];
+    }
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED, class R>
+int do_load_aos(pbpic_handle* h, const RefRec<R>* host, int64_t n) {
+  if (n < 0 || n > h->cap) return fail(PBPIC_ECAPACITY, "particle count exceeds the handle's capacity");
+  const int b = h->cur;
+  if (n > 0) {
+    TRY(ensure_staging(h, (size_t)n * sizeof(RefRec<R>)));
+    CK(cudaMemcpyAsync(h->staging, host, (size_t)n * sizeof(RefRec<R>), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    k_aos_in<T, R><<<grid_for(n, 256), 256, 0, h->stream>>>((const RefRec<R>*)h->staging, n, h->cfg.mx, h->cfg.my,
+                                                              h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
+                                                              P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4),
+                                                              h->pid[b], h->status);
+    CKLAUNCH("k_aos_in");
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (st & 8) return fail(PBPIC_EINVAL, "particle record with grid outside 1..mx*my or q not +-1");
+  }
+  h->n = n;
+  h->itime = 0;
+  TRY(set_unsorted_tiles(h));
+  return kinetic_row<T, MIXED>(h, 0);
+}
+
+template <class T, bool MIXED, class R>
+int do_store_aos(pbpic_handle* h, RefRec<R>* host, int64_t cap, int64_t* nout) {
+  if (nout) *nout = h->n;
+  const int64_t n = std::min<int64_t>(cap, h->n);
+  if (n <= 0) return PBPIC_OK;
+  const int b = h->cur;
+  TRY(ensure_staging(h, (size_t)n * sizeof(RefRec<R>)));
+  k_aos_out<T, R><<<grid_for(n, 256), 256, 0, h->stream>>>((RefRec<R>*)h->staging, n, h->cfg.my, h->cell[b],
+                                                             P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
+                                                             P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b]);
+  CKLAUNCH("k_aos_out");
+  CK(cudaMemcpyAsync(host, h->staging, (size_t)n * sizeof(RefRec<R>), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+pic::LoadParams loader_params(const pbpic_handle* h, const pbpic_loader* ld) {
+  const pbpic_config& c = h->cfg;
+  pic::LoadParams L;
+  memset(&L, 0, sizeof(L));
+  L.kind = ld->kind;
+  L.mx = c.mx;
+  L.my = c.my;
+  L.dx = c.dx;
+  L.dy = c.dy;
+  L.ppc = ld->ppc;
+  L.npairs = (int64_t)ld->ppc * c.mx * c.my;
+  auto u = [](double v) { return v / sqrt(1.0 - v * v); };  // pic2d.f90:383-387
+  L.uthe = u(ld->vthe);
+  L.uthi = u(ld->vthi);
+  L.uthe_perp = L.uthe;
+  if (ld->kind == PBPIC_LOAD_WEIBEL) {
+    const double a = ld->anisotropy > 0 ? ld->anisotropy : 1.0;
+    L.uthe_perp = u(ld->vthe);
+    L.uthe = u(ld->vthe / sqrt(a));
+  }
+  L.udrift_e = u(ld->vdrift_e);
+  L.udrift_i = u(ld->vdrift_i);
+  L.lambda = ld->lambda;
+  L.seed = ld->seed;
+  if (ld->kind == PBPIC_LOAD_HARRIS) {
+    const double Ly = c.my * c.dy;
+    const double fs = 2.0 * ld->lambda / (2.0 * ld->lambda + ld->nb * Ly);
+    L.nsheet = (int64_t)llround((double)L.npairs * fs);
+  }
+  return L;
+}
+
+int validate_loader(const pbpic_handle* h, const pbpic_loader* ld) {
+  if (!ld) return fail(PBPIC_EINVAL, "null loader");
+  if (ld->kind < 0 || ld->kind > 3) return fail(PBPIC_EINVAL, "unknown loader kind");
+  if (ld->ppc <= 0) return fail(PBPIC_EINVAL, "loader ppc must be positive");
+  if (ld->vthe < 0 || ld->vthe >= 1 || ld->vthi < 0 || ld->vthi >= 1) return fail(PBPIC_EINVAL, "thermal speeds must be in [0, c)");
+  if (fabs(ld->vdrift_e) >= 1 || fabs(ld->vdrift_i) >= 1) return fail(PBPIC_EINVAL, "drift speeds must be below c");
+  if (ld->kind == PBPIC_LOAD_HARRIS && (ld->lambda <= 0 || ld->nb < 0))
+    return fail(PBPIC_EINVAL, "Harris loader needs lambda > 0 and nb >= 0");
+  (void)h;
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_init_plasma(pbpic_handle* h, const pbpic_loader* ld) {
+  TRY(validate_loader(h, ld));
+  pic::LoadParams L = loader_params(h, ld);
+  const int64_t n = ld->immobile_ions ? L.npairs : 2 * L.npairs;
+  if (n > h->cap) return fail(PBPIC_ECAPACITY, "loader produces more particles than the capacity");
+  const int b = h->cur;
+  if (L.npairs > 0) {
+    k_load<T><<<(unsigned)((L.npairs + 255) / 256), 256, 0, h->stream>>>(
+        L, L.npairs, ld->immobile_ions, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2), P<T>(h, b, 3),
+        P<T>(h, b, 4), h->pid[b]);
+    CKLAUNCH("k_load");
+  }
+  h->n = n;
+  h->itime = 0;
+  // initial fields (initfields, pic2d.f90:583-648)
+  pic::FieldInit fi;
+  fi.kind = ld->kind;
+  fi.mx = h->cfg.mx;
+  fi.my = h->cfg.my;
+  fi.dx = h->cfg.dx;
+  fi.dy = h->cfg.dy;
+  fi.lambda = ld->lambda;
+  fi.psi0 = ld->psi0;
+  fi.bguide = ld->bguide;
+  fi.b0z = ld->b0z;
+  const int64_t pe = plane_elems(h);
+  std::vector<double> yee((size_t)(6 * pe), 0.0);
+  for (int i = 0; i < fi.mx; ++i)
+    for (int j = 0; j <= fi.my; ++j) {
+      yee[(size_t)3 * pe + (size_t)i * h->S + j] = pic::init_bx(fi, i, j);
+      yee[(size_t)4 * pe + (size_t)i * h->S + j] = pic::init_by(fi, i, j);
+      yee[(size_t)5 * pe + (size_t)i * h->S + j] = pic::init_bz(fi, i, j);
+    }
+  TRY((do_load_fields<T, MIXED>(h, yee.data())));
+  TRY((kinetic_row<T, MIXED>(h, 0)));
+  TRY((do_sort<T, MIXED>(h)));
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_gauss(pbpic_handle* h, double* out) {
+  cudaStream_t s = h->stream;
+  const int64_t pe = plane_elems(h);
+  CK(cudaMemsetAsync(h->rho, 0, (size_t)pe * 8, s));
+  CK(cudaMemsetAsync(h->dscalar, 0, 8, s));
+  const int b = h->cur;
+  if (h->n > 0) {
+    k_rho<T><<<grid_for(h->n, 256), 256, 0, s>>>(h->n, h->cfg.mx, h->cfg.my, h->S, h->cfg.ybc, h->cell[b],
+                                                  P<T>(h, b, 0), P<T>(h, b, 1), h->rho);
+    CKLAUNCH("k_rho");
+  }
+  const pbpic_config& c = h->cfg;
+  k_gauss<T><<<grid_for(pe, 256), 256, 0, s>>>(c.mx, c.my, h->S, c.ybc, (const T*)h->f[0], (const T*)h->f[1],
+                                                h->rho, 1.0 / c.dx, 1.0 / c.dy, 1.0 / (c.cva * c.cva), c.in0,
+                                                h->dscalar);
+  CKLAUNCH("k_gauss");
+  CK(cudaMemcpyAsync(out, h->dscalar, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_flux(pbpic_handle* h, double* out) {
+  k_flux<T><<<1, 256, 0, h->stream>>>(h->cfg.mx, h->cfg.my, (const T*)h->ng, h->cfg.dx, h->dscalar);
+  CKLAUNCH("k_flux");
+  CK(cudaMemcpyAsync(out, h->dscalar, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+#define DISPATCH(h, FN, ...) ((h)->mixed ? FN<float, true>(__VA_ARGS__) : FN<double, false>(__VA_ARGS__))
+
+int check_handle(const pbpic_handle* h) {
+  if (!h) return fail(PBPIC_EINVAL, "null handle");
+  return PBPIC_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* pbpic_last_error(void) { return g_err.c_str(); }
+
+int pbpic_kernel_launches(int64_t* count) {
+  if (!count) return fail(PBPIC_EINVAL, "null argument");
+  *count = g_launches.load(std::memory_order_relaxed);
+  return PBPIC_OK;
+}
+
+int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
+  if (!cfg || !out) return fail(PBPIC_EINVAL, "null argument");
+  *out = nullptr;
+  const pbpic_config& c = *cfg;
+  if (c.mx < 2 || c.my < 2 || c.mx > 32767 || c.my > 65535)
+    return fail(PBPIC_EINVAL, "mx must be in [2, 32767] and my in [2, 65535]");
+  if ((int64_t)c.mx * c.my > (1ll << 30)) return fail(PBPIC_EINVAL, "mx*my must not exceed 2^30 cells");
+  if (!(c.dx > 0 && c.dy > 0 && c.dt > 0 && c.cva > 0 && c.mime > 0 && c.in0 > 0))
+    return fail(PBPIC_EINVAL, "dx, dy, dt, cva, mime and in0 must be positive");
+  if (c.ybc != PBPIC_BC_PERIODIC && c.ybc != PBPIC_BC_CONDUCTING) return fail(PBPIC_EINVAL, "unknown ybc");
+  if (c.precision != PBPIC_FP64_PLAIN && c.precision != PBPIC_FP32_MIXED)
+    return fail(PBPIC_EINVAL, "unknown precision");
+  if (c.capacity < 0 || c.capacity > 0x7fffff00ll) return fail(PBPIC_EINVAL, "capacity must be in [0, 2^31)");
+  if (c.compat & ~7) return fail(PBPIC_EINVAL, "unknown compat bits");
+  const double cfl = c.cva * c.dt * sqrt(1.0 / (c.dx * c.dx) + 1.0 / (c.dy * c.dy));
+  if (!(cfl < 1.0)) return fail(PBPIC_EINVAL, "time step violates the CFL condition c*dt*sqrt(1/dx^2+1/dy^2) < 1");
+  if (c.cva * c.dt / std::min(c.dx, c.dy) >= 1.0)
+    return fail(PBPIC_EINVAL, "a particle at c would cross more than one cell per step");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(PBPIC_ECUDA, "no CUDA device");
+  pbpic_handle* h = new pbpic_handle();
+  h->cfg = c;
+  h->mixed = c.precision == PBPIC_FP32_MIXED;
+  h->tsz = h->mixed ? 4 : 8;
+  h->S = c.my + 1;
+  h->ncells = c.mx * c.my;
+  h->TY = c.tile_rows > 0 ? std::min(c.tile_rows, c.my) : std::min(c.my, 32);
+  h->tpc = (c.my + h->TY - 1) / h->TY;
+  h->ntiles = c.mx * h->tpc;
+  h->cap = c.capacity;
+  const size_t capn = (size_t)std::max<int64_t>(c.capacity, 1);
+  const int64_t pe = plane_elems(h);
+  int r = PBPIC_OK;
+  auto A = [&](auto** p, size_t bytes) {
+    if (r == PBPIC_OK) r = dalloc(h, p, bytes);
+  };
+  for (int b = 0; b < 2; ++b) {
+    A(&h->cell[b], capn * 4);
+    for (int k = 0; k < 5; ++k) A(&h->comp[b][k], capn * h->tsz);
+    if (c.track_pid) A(&h->pid[b], capn * 4);
+    A(&h->keys[b], capn * 4);
+    A(&h->vals[b], capn * 4);
+  }
+  for (int k = 0; k < 6; ++k) A(&h->f[k], (size_t)pe * h->tsz);
+  A(&h->ng, (size_t)(c.mx + 1) * (c.my + 1) * 8 * h->tsz);
+  A(&h->jacc, (size_t)4 * pe * 8);
+  A(&h->counts, (size_t)(h->ncells + 1) * 4);
+  A(&h->off, (size_t)(h->ncells + 1) * 4);
+  A(&h->tile_off, (size_t)(h->ntiles + 1) * 4);
+  A(&h->ke_part, (size_t)std::max(h->ntiles, 148 * 16) * 2 * 8);
+  h->nke = 148 * 8;
+  h->nfe = grid_for((int64_t)(c.mx + 1) * (c.my + 1), 256, 148 * 8);
+  A(&h->fe_part, (size_t)h->nfe * 2 * 8);
+  A(&h->status, 16);
+  A(&h->rhist, (size_t)radix_hist_ints((int64_t)capn) * 4);
+  const int64_t sc = std::max(scan_scratch_ints(radix_hist_ints((int64_t)capn)), scan_scratch_ints(h->ncells + 1));
+  A(&h->scan_scratch, (size_t)sc * 4);
+  A(&h->rho, (size_t)pe * 8);
+  A(&h->dscalar, 16);
+  if (r != PBPIC_OK) {
+    pbpic_destroy(h);
+    return r;
+  }
+  for (int k = 0; k < 6; ++k) cudaMemset(h->f[k], 0, (size_t)pe * h->tsz);
+  cudaMemset(h->ng, 0, (size_t)(c.mx + 1) * (c.my + 1) * 8 * h->tsz);
+  cudaMemset(h->jacc, 0, (size_t)4 * pe * 8);
+  cudaMemset(h->counts, 0, (size_t)(h->ncells + 1) * 4);
+  cudaMemset(h->off, 0, (size_t)(h->ncells + 1) * 4);
+  cudaMemset(h->status, 0, 16);
+  if (ensure_hist(h, 64) != PBPIC_OK || set_unsorted_tiles(h) != PBPIC_OK) {
+    pbpic_destroy(h);
+    return PBPIC_ENOMEM;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    pbpic_destroy(h);
+    return fail(PBPIC_ECUDA, "device initialisation failed");
+  }
+  *out = h;
+  return PBPIC_OK;
+}
+
+int pbpic_destroy(pbpic_handle* h) {
+  if (!h) return PBPIC_OK;
+  cudaStreamSynchronize(h->stream);
+  for (void* p : h->allocs) cudaFree(p);
+  delete h;
+  return PBPIC_OK;
+}
+
+int pbpic_set_stream(pbpic_handle* h, void* stream) {
+  TRY(check_handle(h));
+  h->stream = (cudaStream_t)stream;
+  return PBPIC_OK;
+}
+
+int pbpic_get_config(const pbpic_handle* h, pbpic_config* out) {
+  TRY(check_handle(h));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  *out = h->cfg;
+  return PBPIC_OK;
+}
+
+int pbpic_loader_count(const pbpic_handle* h, const pbpic_loader* ld, int64_t* n) {
+  TRY(check_handle(h));
+  TRY(validate_loader(h, ld));
+  if (!n) return fail(PBPIC_EINVAL, "null argument");
+  const int64_t pairs = (int64_t)ld->ppc * h->cfg.mx * h->cfg.my;
+  *n = ld->immobile_ions ? pairs : 2 * pairs;
+  return PBPIC_OK;
+}
+
+int pbpic_init_plasma(pbpic_handle* h, const pbpic_loader* ld) {
+  TRY(check_handle(h));
+  return DISPATCH(h, do_init_plasma, h, ld);
+}
+
+int pbpic_load_particles_f32(pbpic_handle* h, const pbpic_particle_f32* p, int64_t n) {
+  TRY(check_handle(h));
+  if (!p && n > 0) return fail(PBPIC_EINVAL, "null particles");
+  const RefRec<float>* r = reinterpret_cast<const RefRec<float>*>(p);
+  return h->mixed ? do_load_aos<float, true, float>(h, r, n) : do_load_aos<double, false, float>(h, r, n);
+}
+
+int pbpic_load_particles_f64(pbpic_handle* h, const pbpic_particle_f64* p, int64_t n) {
+  TRY(check_handle(h));
+  if (!p && n > 0) return fail(PBPIC_EINVAL, "null particles");
+  const RefRec<double>* r = reinterpret_cast<const RefRec<double>*>(p);
+  return h->mixed ? do_load_aos<float, true, double>(h, r, n) : do_load_aos<double, false, double>(h, r, n);
+}
+
+int pbpic_store_particles_f32(pbpic_handle* h, pbpic_particle_f32* p, int64_t cap, int64_t* n) {
+  TRY(check_handle(h));
+  if (!p && cap > 0) return fail(PBPIC_EINVAL, "null particles");
+  RefRec<float>* r = reinterpret_cast<RefRec<float>*>(p);
+  return h->mixed ? do_store_aos<float, true, float>(h, r, cap, n) : do_store_aos<double, false, float>(h, r, cap, n);
+}
+
+int pbpic_store_particles_f64(pbpic_handle* h, pbpic_particle_f64* p, int64_t cap, int64_t* n) {
+  TRY(check_handle(h));
+  if (!p && cap > 0) return fail(PBPIC_EINVAL, "null particles");
+  RefRec<double>* r = reinterpret_cast<RefRec<double>*>(p);
+  return h->mixed ? do_store_aos<float, true, double>(h, r, cap, n)
+                  : do_store_aos<double, false, double>(h, r, cap, n);
+}
+
+int pbpic_load_particles_soa_f64(pbpic_handle* h, int64_t n, const int32_t* grid, const int32_t* q,
+                                 const double* dx, const double* dy, const double* ux, const double* uy,
+                                 const double* uz, const int32_t* pid) {
+  TRY(check_handle(h));
+  if (n > 0 && !(grid && q && dx && dy && ux && uy && uz)) return fail(PBPIC_EINVAL, "null array");
+  std::vector<pbpic_particle_f64> tmp((size_t)std::max<int64_t>(n, 0));
+  for (int64_t i = 0; i < n; ++i)
+    tmp[i] = pbpic_particle_f64{dx[i], dy[i], ux[i], uy[i], uz[i], grid[i], q[i], pid ? pid[i] : 0, 0};
+  return pbpic_load_particles_f64(h, tmp.data(), n);
+}
+
+int pbpic_store_particles_soa_f64(pbpic_handle* h, int64_t cap, int64_t* n, int32_t* grid, int32_t* q, double* dx,
+                                  double* dy, double* ux, double* uy, double* uz, int32_t* pid) {
+  TRY(check_handle(h));
+  int64_t m = std::min<int64_t>(cap, h->n);
+  std::vector<pbpic_particle_f64> tmp((size_t)std::max<int64_t>(m, 0));
+  TRY(pbpic_store_particles_f64(h, tmp.data(), m, nullptr));
+  if (n) *n = h->n;
+  for (int64_t i = 0; i < m; ++i) {
+    if (grid) grid[i] = tmp[i].grid;
+    if (q) q[i] = tmp[i].q;
+    if (dx) dx[i] = tmp[i].dx;
+    if (dy) dy[i] = tmp[i].dy;
+    if (ux) ux[i] = tmp[i].ux;
+    if (uy) uy[i] = tmp[i].uy;
+    if (uz) uz[i] = tmp[i].uz;
+    if (pid) pid[i] = tmp[i].pid;
+  }
+  return PBPIC_OK;
+}
+
+int pbpic_num_particles(const pbpic_handle* h, int64_t* n) {
+  TRY(check_handle(h));
+  if (!n) return fail(PBPIC_EINVAL, "null argument");
+  *n = h->n;
+  return PBPIC_OK;
+}
+
+int pbpic_load_fields_f64(pbpic_handle* h, const double* yee6) {
+  TRY(check_handle(h));
+  if (!yee6) return fail(PBPIC_EINVAL, "null fields");
+  return DISPATCH(h, do_load_fields, h, yee6);
+}
+
+int pbpic_store_fields_f64(pbpic_handle* h, double* yee6) {
+  TRY(check_handle(h));
+  if (!yee6) return fail(PBPIC_EINVAL, "null fields");
+  return DISPATCH(h, do_store_fields, h, yee6);
+}
+
+int pbpic_store_emfgrid_f64(pbpic_handle* h, double* grid8) {
+  TRY(check_handle(h));
+  if (!grid8) return fail(PBPIC_EINVAL, "null buffer");
+  return DISPATCH(h, do_store_grid, h, grid8);
+}
+
+int pbpic_store_denjr_f64(pbpic_handle* h, double* j4) {
+  TRY(check_handle(h));
+  if (!j4) return fail(PBPIC_EINVAL, "null buffer");
+  return do_store_denjr(h, j4);
+}
+
+int pbpic_push(pbpic_handle* h) {
+  TRY(check_handle(h));
+  return DISPATCH(h, do_push, h);
+}
+
+int pbpic_fieldsolve(pbpic_handle* h) {
+  TRY(check_handle(h));
+  return DISPATCH(h, do_fieldsolve, h);
+}
+
+int pbpic_sort(pbpic_handle* h) {
+  TRY(check_handle(h));
+  return DISPATCH(h, do_sort, h);
+}
+
+int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every) {
+  TRY(check_handle(h));
+  if (nsteps < 0 || sort_every < 0) return fail(PBPIC_EINVAL, "nsteps and sort_every must be >= 0");
+  for (int s = 0; s < nsteps; ++s) {
+    TRY(pbpic_push(h));
+    TRY(pbpic_fieldsolve(h));
+    if (sort_every > 0 && h->itime % sort_every == 0) TRY(pbpic_sort(h));
+  }
+  return PBPIC_OK;
+}
+
+int pbpic_synchronize(pbpic_handle* h) {
+  TRY(check_handle(h));
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+int pbpic_energies(pbpic_handle* h, double out[4]) {
+  TRY(check_handle(h));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  CK(cudaMemcpyAsync(out, h->hist + (size_t)h->itime * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+int pbpic_energy_history(pbpic_handle* h, double* out, int32_t max_rows, int32_t* n_rows) {
+  TRY(check_handle(h));
+  const int rows = std::min(max_rows, h->itime + 1);
+  if (n_rows) *n_rows = h->itime + 1;
+  if (rows > 0) {
+    if (!out) return fail(PBPIC_EINVAL, "null buffer");
+    CK(cudaMemcpyAsync(out, h->hist, (size_t)rows * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return PBPIC_OK;
+}
+
+int pbpic_time_step(const pbpic_handle* h, int32_t* itime) {
+  TRY(check_handle(h));
+  if (!itime) return fail(PBPIC_EINVAL, "null argument");
+  *itime = h->itime;
+  return PBPIC_OK;
+}
+
+int pbpic_cell_counts(pbpic_handle* h, int32_t* counts) {
+  TRY(check_handle(h));
+  if (!counts) return fail(PBPIC_EINVAL, "null buffer");
+  CK(cudaMemcpyAsync(counts, h->counts, (size_t)h->ncells * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+int pbpic_gauss_residual(pbpic_handle* h, double* out) {
+  TRY(check_handle(h));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  return DISPATCH(h, do_gauss, h, out);
+}
+
+int pbpic_reconnected_flux(pbpic_handle* h, double* out) {
+  TRY(check_handle(h));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  return DISPATCH(h, do_flux, h, out);
+}
+
+int pbpic_status(pbpic_handle* h, int32_t* bits) {
+  TRY(check_handle(h));
+  if (!bits) return fail(PBPIC_EINVAL, "null argument");
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *bits = st;
+  return PBPIC_OK;
+}
+
+int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells, int32_t* perm_dev,
+                             int32_t* counts_dev, void* stream) {
+  if (n < 0 || n > 0x7fffff00ll || ncells <= 0) return fail(PBPIC_EINVAL, "bad n or ncells");
+  if (n > 0 && (!keys_dev || !perm_dev)) return fail(PBPIC_EINVAL, "null device buffer");
+  if (!counts_dev) return fail(PBPIC_EINVAL, "null counts buffer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nn = (size_t)std::max<int64_t>(n, 1);
+  const int64_t rh = radix_hist_ints((int64_t)nn);
+  const int64_t sc = std::max(scan_scratch_ints(rh), (int64_t)16);
+  const size_t bytes = nn * 4 * 4 + (size_t)rh * 4 + (size_t)sc * 4 + 16;
+  char* buf = nullptr;
+  CK(cudaMallocAsync((void**)&buf, bytes, s));
+  int32_t* k0 = (int32_t*)buf;
+  int32_t* k1 = k0 + nn;
+  int32_t* v0 = k1 + nn;
+  int32_t* v1 = v0 + nn;
+  int32_t* rhist = v1 + nn;
+  int32_t* scr = rhist + rh;
+  int* status = (int*)(scr + sc);
+  int rc = PBPIC_OK;
+  int st = 0;
+  do {
+    if (cudaMemsetAsync(counts_dev, 0, (size_t)ncells * 4, s) != cudaSuccess ||
+        cudaMemsetAsync(status, 0, 4, s) != cudaSuccess) {
+      rc = fail(PBPIC_ECUDA, "cudaMemsetAsync failed");
+      break;
+    }
+    if (n == 0) break;
+    k_key_hist<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(keys_dev, n, ncells, counts_dev, status);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaGetLastError() != cudaSuccess) {
+      rc = fail(PBPIC_ECUDA, "k_key_hist launch failed");
+      break;
+    }
+    if (cudaMemcpyAsync(k0, keys_dev, (size_t)n * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+      rc = fail(PBPIC_ECUDA, "key copy failed");
+      break;
+    }
+    int32_t* perm = nullptr;
+    rc = radix_sort(s, n, ncells, k0, k1, v0, v1, rhist, scr, &perm);
+    if (rc != PBPIC_OK) break;
+    if (cudaMemcpyAsync(perm_dev, perm, (size_t)n * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+      rc = fail(PBPIC_ECUDA, "permutation copy failed");
+      break;
+    }
+  } while (0);
+  if (cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess && rc == PBPIC_OK)
+    rc = fail(PBPIC_ECUDA, "status copy failed");
+  cudaFreeAsync(buf, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess && rc == PBPIC_OK) rc = fail(PBPIC_ECUDA, "stream synchronize failed");
+  if (rc == PBPIC_OK && (st & 8)) rc = fail(PBPIC_EINVAL, "key outside [0, ncells)");
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+"""Host-side view of one pbpic domain on the GPU, over the C ABI.
+
+The methods keep the names of the reference's subroutines
+(src/programs/pic2d.f90): `pusher` (912-1217), `fieldsolver` (678-860),
+`countingsort` (1303-1329), and the time loop body `step` (171-188). Errors
+of the library raise PbpicError with the library's message.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+
+class Simulation:
+    def __init__(self, mx, my, dx, dy, dt, cva, mime, in0, ybc=L.BC_PERIODIC, precision="fp64",
+                 compat=0, track_pid=False, capacity=0, tile_rows=0):
+        self._lib = L.lib()
+        prec = {"fp64": L.FP64_PLAIN, "plain": L.FP64_PLAIN, "fp32": L.FP32_MIXED, "mixed": L.FP32_MIXED}[precision]
+        self.cfg = L.Config(mx=mx, my=my, dx=dx, dy=dy, dt=dt, cva=cva, mime=mime, in0=in0, ybc=ybc,
+                            precision=prec, compat=compat, track_pid=int(bool(track_pid)),
+                            capacity=int(capacity), tile_rows=tile_rows)
+        self.mx, self.my = mx, my
+        self.precision = precision
+        self._h = ctypes.c_void_p()
+        L.check(self._lib.pbpic_create(ctypes.byref(self.cfg), ctypes.byref(self._h)))
+
+    @classmethod
+    def from_config(cls, cfg, **kw):
+        args = dict(cfg)
+        args.update(kw)
+        return cls(**args)
+
+    # --------------------------------------------------------------- lifecycle
+    def close(self):
+        if self._h:
+            self._lib.pbpic_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr):
+        L.check(self._lib.pbpic_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    # ----------------------------------------------------------------- loading
+    @staticmethod
+    def loader(**kw):
+        ld = L.Loader()
+        for k, v in kw.items():
+            setattr(ld, k, v)
+        return ld
+
+    def loader_count(self, **kw):
+        n = ctypes.c_int64()
+        L.check(self._lib.pbpic_loader_count(self._h, ctypes.byref(self.loader(**kw)), ctypes.byref(n)))
+        return n.value
+
+    def init_plasma(self, **kw):
+        L.check(self._lib.pbpic_init_plasma(self._h, ctypes.byref(self.loader(**kw))))
+
+    def load_particles(self, p):
+        p = np.ascontiguousarray(p)
+        if p.dtype == L.PARTICLE_F32:
+            L.check(self._lib.pbpic_load_particles_f32(self._h, L.ptr(p), len(p)))
+        elif p.dtype == L.PARTICLE_F64:
+            L.check(self._lib.pbpic_load_particles_f64(self._h, L.ptr(p), len(p)))
+        else:
+            raise TypeError("particles must have dtype PARTICLE_F32 or PARTICLE_F64")
+
+    def num_particles(self):
+        n = ctypes.c_int64()
+        L.check(self._lib.pbpic_num_particles(self._h, ctypes.byref(n)))
+        return n.value
+
+    def particles(self, dtype=L.PARTICLE_F64):
+        n = self.num_particles()
+        out = np.zeros(n, dtype=dtype)
+        got = ctypes.c_int64()
+        fn = self._lib.pbpic_store_particles_f64 if dtype == L.PARTICLE_F64 else self._lib.pbpic_store_particles_f32
+        L.check(fn(self._h, L.ptr(out), n, ctypes.byref(got)))
+        return out
+
+    def load_fields(self, yee6):
+        a = np.ascontiguousarray(yee6, dtype=np.float64)
+        assert a.shape == (6, self.mx, self.my + 1)
+        L.check(self._lib.pbpic_load_fields_f64(self._h, L.ptr(a)))
+
+    def fields(self):
+        a = np.zeros((6, self.mx, self.my + 1))
+        L.check(self._lib.pbpic_store_fields_f64(self._h, L.ptr(a)))
+        return a
+
+    def emfgrid(self):
+        a = np.zeros((self.mx + 1, self.my + 1, 8))
+        L.check(self._lib.pbpic_store_emfgrid_f64(self._h, L.ptr(a)))
+        return a
+
+    def denjr(self):
+        a = np.zeros((4, self.mx, self.my + 1))
+        L.check(self._lib.pbpic_store_denjr_f64(self._h, L.ptr(a)))
+        return a
+
+    # -------------------------------------------------------------------- step
+    def pusher(self):
+        L.check(self._lib.pbpic_push(self._h))
+
+    def fieldsolver(self):
+        L.check(self._lib.pbpic_fieldsolve(self._h))
+
+    def countingsort(self):
+        L.check(self._lib.pbpic_sort(self._h))
+
+    def step(self, nsteps=1, sort_every=50):
+        L.check(self._lib.pbpic_step(self._h, nsteps, sort_every))
+
+    def synchronize(self):
+        L.check(self._lib.pbpic_synchronize(self._h))
+
+    # ------------------------------------------------------------- diagnostics
+    def energies(self):
+        a = np.zeros(4)
+        L.check(self._lib.pbpic_energies(self._h, L.ptr(a)))
+        return a
+
+    def energy_history(self):
+        n = ctypes.c_int32()
+        L.check(self._lib.pbpic_energy_history(self._h, None, 0, ctypes.byref(n)))
+        a = np.zeros((n.value, 4))
+        L.check(self._lib.pbpic_energy_history(self._h, L.ptr(a), n.value, ctypes.byref(n)))
+        return a
+
+    def itime(self):
+        t = ctypes.c_int32()
+        L.check(self._lib.pbpic_time_step(self._h, ctypes.byref(t)))
+        return t.value
+
+    def cell_counts(self):
+        a = np.zeros(self.mx * self.my, dtype=np.int32)
+        L.check(self._lib.pbpic_cell_counts(self._h, L.ptr(a)))
+        return a
+
+    def gauss_residual(self):
+        v = ctypes.c_double()
+        L.check(self._lib.pbpic_gauss_residual(self._h, ctypes.byref(v)))
+        return v.value
+
+    def reconnected_flux(self):
+        v = ctypes.c_double()
+        L.check(self._lib.pbpic_reconnected_flux(self._h, ctypes.byref(v)))
+        return v.value
+
+    def status(self):
+        v = ctypes.c_int32()
+        L.check(self._lib.pbpic_status(self._h, ctypes.byref(v)))
+        return v.value
+
+
+def counting_sort_keys(keys_ptr, n, ncells, perm_ptr, counts_ptr, stream_ptr=0):
+    """Stateless stable counting sort on device buffers (raw pointers)."""
+    lib = L.lib()
+    L.check(lib.pbpic_counting_sort_keys(ctypes.c_void_p(keys_ptr), n, ncells, ctypes.c_void_p(perm_ptr),
+                                         ctypes.c_void_p(counts_ptr), ctypes.c_void_p(stream_ptr)))
+
+
+def kernel_launches():
+    """Kernels launched by the library in this process so far."""
+    n = ctypes.c_int64()
+    L.check(L.lib().pbpic_kernel_launches(ctypes.byref(n)))
+    return n.value

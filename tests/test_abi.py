@@ -1,0 +1,69 @@
+"""The C ABI library builds for sm_100a, loads without a GPU, exports every
+function include/pbpic.h declares, and its structs match the Python views
+(CPU; no compute calls)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pbpic.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pbpic_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_step_boundary():
+    names = declared_functions()
+    for need in ("pbpic_create", "pbpic_destroy", "pbpic_push", "pbpic_fieldsolve", "pbpic_sort", "pbpic_step",
+                 "pbpic_energies", "pbpic_gauss_residual", "pbpic_load_particles_f32", "pbpic_store_particles_f32",
+                 "pbpic_load_fields_f64", "pbpic_store_denjr_f64", "pbpic_last_error"):
+        assert need in names
+
+
+def test_library_exports_every_declared_symbol():
+    from pbpic_b200 import build
+    lib_path = build.build()
+    lib = ctypes.CDLL(lib_path)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_the_header():
+    from pbpic_b200 import _lib
+    declared = set(declared_functions()) - {"pbpic_last_error"}
+    assert declared == set(_lib.SIGNATURES)
+
+
+def test_struct_layouts_match_c(tmp_path):
+    from pbpic_b200 import _lib
+    src = tmp_path / "sz.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "pbpic.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(pbpic_config), sizeof(pbpic_loader),"
+        " sizeof(pbpic_particle_f32), sizeof(pbpic_particle_f64), offsetof(pbpic_config, capacity),"
+        " offsetof(pbpic_loader, seed));return 0;}\n")
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == [ctypes.sizeof(_lib.Config), ctypes.sizeof(_lib.Loader), _lib.PARTICLE_F32.itemsize,
+                   _lib.PARTICLE_F64.itemsize, _lib.Config.capacity.offset, _lib.Loader.seed.offset]
+
+
+def test_create_reports_errors_without_crashing():
+    """Invalid configurations are rejected with a message before any device work."""
+    import pbpic_b200
+    from pbpic_b200 import configs
+    cfg, _ = configs.uniform_c1(mx=8, my=8)
+    bad = dict(cfg, mx=1)
+    with pytest.raises(pbpic_b200.PbpicError) as e:
+        pbpic_b200.Simulation(**bad)
+    assert "mx" in str(e.value)
+    with pytest.raises(pbpic_b200.PbpicError) as e:
+        pbpic_b200.Simulation(**dict(cfg, dt=cfg["dt"] * 4))
+    assert "CFL" in str(e.value)
