@@ -83,9 +83,16 @@ def harris_c5(seed=4):
     return harris(4096, 2048, 100, seed, mime=100.0, nb=0.1, bguide=0.2, dx=0.05)
 
 
+def harris_mid(seed=1):
+    """The Harris sheet of harris_c2 on a quarter of the cells (512x256, ~26M
+    particles): the profiling case, still far larger than L2."""
+    return harris(512, 256, 100, seed)
+
+
 WORKLOADS = {
     "uniform_128x128_ppc32": uniform_c1,
     "harris_1024x512_ppc100": harris_c2,
+    "harris_512x256_ppc100": harris_mid,
     "harris_256x128_ppc64": harris_c4,
     "harris_4096x2048_ppc100": harris_c5,
 }

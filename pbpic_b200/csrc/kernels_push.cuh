@@ -4,21 +4,34 @@
 // currentdeposit (pic2d.f90:1226-1296).
 //
 // Work decomposition: a tile is a run of `tile_rows` cells of one column
-// (cells ix*my + y0 .. ix*my + y0 + tile_rows - 1, contiguous in the sorted
-// order), and one block pushes the particles of one tile. Its current goes to
-// a shared-memory window of 4 node columns (ix-1 .. ix+2) x (tile_rows + 3)
-// node rows, which covers every node a particle of the tile can touch in one
-// step. Non-crossing particles deposit a 17-value stencil relative to their
-// cell; lanes of a warp that share a cell are summed by a segmented scan and
-// only the last lane of each run adds to shared memory. Crossing particles add
-// their 16 values individually. A particle outside its tile (the array is not
-// sorted) adds straight to global memory. At the end the window is folded into
-// the global current with the periodic wrap and the wall images.
+// (contiguous in the cell-sorted order); one block pushes the particles of one
+// tile. Each thread takes 4 consecutive particles per pass, read and written
+// with 128-bit accesses. Consecutive particles of a sorted array share their
+// cell, so a thread keeps the 4 gather nodes of its current cell in registers
+// and sums the deposit stencils of its particles before touching memory.
+//
+// Deposit: the zig-zag move of a particle splits at the relay point into a
+// segment in the old cell and one in the new cell. Everything attached to the
+// old cell -- the first segment's jx/jy (and the second's when the particle
+// does not cross), jz on the 3x3 nodes around the cell, rho -- forms a
+// 17-value stencil. Threads of a warp that share a cell are summed by a
+// segmented scan, and the sum of each run is added to a shared-memory window
+// by 17 lanes at once. A crossing particle adds its second segment (4 values)
+// on its own. The window (4 node columns x tile_rows + 3 node rows) is folded
+// into the global current at the end, with the periodic wrap and the wall
+// images. Particles outside their tile (array not sorted) add straight to
+// global memory.
+//
+// With HIST the kernel also counts the new cells of its particles in the
+// tile's window (the 3x3 neighbourhood of the tile), the first half of the
+// fused counting sort (kernels_sort.cuh).
 #pragma once
 #include <type_traits>
 #include "device_common.cuh"
 
 namespace pbd {
+
+constexpr int PPT = 4;  // particles per thread per pass
 
 template <class T>
 struct PushParams {
@@ -27,8 +40,9 @@ struct PushParams {
   const int32_t* tile_off;  // [ntiles + 1] particle position ranges of the tiles
   uint32_t* cell;
   T *dx, *dy, *ux, *uy, *uz;
-  const T* ng;  // node fields (mx+1) x (my+1) x 8: ex ey ez 0 bx by bz 0
-  void* jacc;   // 4 planes (jx, jy, jz, rho) of mx x S accumulators
+  const T* ng;      // node fields (mx+1) x (my+1) x 8: ex ey ez 0 bx by bz 0
+  void* jacc;       // 4 planes (jx, jy, jz, rho) of mx x S accumulators
+  int32_t* tilecnt; // [ntiles][3*(tile_rows+2)] new-cell counts (HIST)
   T c0[2], c1[2], ms[2], qx[2], qy[2], q[2];  // per species: 0 ion, 1 electron
   T dtcva, idx, idy, cva;
   double* ke_part;  // [ntiles][2]: electron, ion kinetic energy of the tile
@@ -51,27 +65,53 @@ __device__ __forceinline__ Node6<double> load_node(const double* g) {
   return Node6<double>{a.x, a.y, b.x, c.x, c.y, d.x};
 }
 
-// State of one particle after the push, and its 16 deposit terms.
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const uint32_t* p, uint32_t (&v)[4]) {
+  const uint4 x = *reinterpret_cast<const uint4*>(p);
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void st4(uint32_t* p, const uint32_t (&v)[4]) {
+  *reinterpret_cast<uint4*>(p) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+// Reciprocal square root and quotient of the push. Plain form: correctly
+// rounded, as the reference's expressions. Mixed form: the hardware
+// reciprocal square root and fast division (deterministic, about 2 ulp).
+__device__ __forceinline__ float push_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ float push_fdiv(float a, float b) { return __fdividef(a, b); }
+
+// Outcome of pushing one particle.
 template <class T>
 struct Pushed {
-  uint32_t cw;          // new cell word
-  T dx, dy, ux, uy, uz; // new state (after reflection)
-  int ix, iy;           // old cell
-  int dcx, dcy, di, dj; // cell steps and jz quadrant
-  T e[16];              // jx 4, jy 4, jz 4, rho 4 (see deposit_terms)
+  uint32_t cw;           // new cell word
+  T dx, dy, ux, uy, uz;  // new state (after reflection)
+  int dcx, dcy, di, dj;  // cell steps and jz quadrant
+  T e[16];               // deposit terms: jx 4, jy 4, jz 4, rho 4
   double ke;
   int status;
 };
 
-// The push of one particle. `MIXED` selects fused multiply-adds; with
-// MIXED == false every expression is evaluated in the reference's order with
-// separately rounded operations.
+// Push of one particle whose gather nodes are n00 (ix,iy), n01 (ix,iy+1),
+// n10 (ix+1,iy), n11 (ix+1,iy+1). MIXED is only instantiated with T = float.
 template <class T, bool MIXED>
-__device__ __forceinline__ void push_one(const PushParams<T>& a, uint32_t w, T px, T py, T pux,
-                                         T puy, T puz, Pushed<T>& o) {
+__device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux,
+                                         T puy, T puz, const Node6<T>& n00, const Node6<T>& n01,
+                                         const Node6<T>& n10, const Node6<T>& n11, Pushed<T>& o) {
   using A = M<T, MIXED>;
-  const int sp = cw_sp(w);
-  const int ix = cw_ix(w), iy = cw_iy(w);
   const T half = T(0.5), one = T(1);
   // CIC weights, pic2d.f90:948-951
   const T axw = A::add(half, px), ayw = A::add(half, py);
@@ -79,23 +119,28 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, uint32_t w, T p
   const T s2 = A::sub(axw, s1);
   const T s3 = A::sub(ayw, s1);
   const T s4 = A::sub(A::sub(A::sub(one, s1), s2), s3);
-  // gather, pic2d.f90:952-963 (nodes ix..ix+1, iy..iy+1)
-  const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
-  const T* g10 = g00 + (long long)(a.my + 1) * 8;
-  const Node6<T> n00 = load_node(g00), n01 = load_node(g00 + 8);
-  const Node6<T> n10 = load_node(g10), n11 = load_node(g10 + 8);
-#define PBD_GATHER(f) \
-  A::mad(n11.f, s1, A::mad(n01.f, s3, A::mad(n10.f, s2, A::mul(n00.f, s4))))
+  // gather, pic2d.f90:952-963, summed in the reference's order
+#define PBD_GATHER(f) A::mad(n11.f, s1, A::mad(n01.f, s3, A::mad(n10.f, s2, A::mul(n00.f, s4))))
   const T ex = PBD_GATHER(ex), ey = PBD_GATHER(ey), ez = PBD_GATHER(ez);
   const T bx = PBD_GATHER(bx), by = PBD_GATHER(by), bz = PBD_GATHER(bz);
 #undef PBD_GATHER
   // Boris rotation, pic2d.f90:969-996
   const T c0 = sp ? a.c0[1] : a.c0[0], c1 = sp ? a.c1[1] : a.c1[0];
   const T umx = A::mad(c1, ex, pux), umy = A::mad(c1, ey, puy), umz = A::mad(c1, ez, puz);
-  T gama = A::sqrt(A::mad(umz, umz, A::mad(umy, umy, A::mad(umx, umx, one))));
-  const T c2 = A::div(c0, gama);
+  const T g2m = A::mad(umz, umz, A::mad(umy, umy, A::mad(umx, umx, one)));
+  T c2, t2;
+  if constexpr (MIXED) {
+    c2 = A::mul(c0, push_rsqrt(g2m));
+  } else {
+    c2 = A::div(c0, A::sqrt(g2m));
+  }
   const T tx = A::mul(c2, bx), ty = A::mul(c2, by), tz = A::mul(c2, bz);
-  const T t2 = A::div(T(2), A::mad(tz, tz, A::mad(ty, ty, A::mad(tx, tx, one))));
+  const T tsq1 = A::mad(tz, tz, A::mad(ty, ty, A::mad(tx, tx, one)));
+  if constexpr (MIXED) {
+    t2 = push_fdiv(T(2), tsq1);
+  } else {
+    t2 = A::div(T(2), tsq1);
+  }
   const T sx = A::mul(t2, tx), sy = A::mul(t2, ty), sz = A::mul(t2, tz);
   const bool cb = (a.compat & 1) != 0;  // rotate the pre-kick momentum (pic2d.f90:985-987)
   const T vx = cb ? pux : umx, vy = cb ? puy : umy, vz0 = cb ? puz : umz;
@@ -106,10 +151,19 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, uint32_t w, T p
   const T upy = A::add(umy, A::mad(u0z, sx, -A::mul(u0x, sz)));
   const T upz = A::add(umz, A::mad(u0x, sy, -A::mul(u0y, sx)));
   const T ux = A::mad(c1, ex, upx), uy = A::mad(c1, ey, upy), uz = A::mad(c1, ez, upz);
-  const T usq = A::mad(uz, uz, A::mad(uy, uy, A::mul(ux, ux)));
-  gama = A::sqrt(A::mad(uz, uz, A::mad(uy, uy, A::mad(ux, ux, one))));
-  // move, pic2d.f90:1002-1023
-  const T c3 = A::div(a.dtcva, gama);
+  const T g2 = A::mad(uz, uz, A::mad(uy, uy, A::mad(ux, ux, one)));
+  T c3, vz, gama;
+  if constexpr (MIXED) {
+    const T rg = push_rsqrt(g2);
+    gama = A::mul(g2, rg);
+    c3 = A::mul(a.dtcva, rg);
+    vz = A::mul(uz, rg);  // uz/gamma; cva enters when the fixed-point sum is converted
+  } else {
+    gama = A::sqrt(g2);
+    c3 = A::div(a.dtcva, gama);            // pic2d.f90:1004
+    vz = A::div(A::mul(uz, a.cva), gama);  // pic2d.f90:1028
+  }
+  // move, pic2d.f90:1005-1023
   const T dx1 = A::mad(A::mul(c3, ux), a.idx, px);
   const T dy1 = A::mad(A::mul(c3, uy), a.idy, py);
   int dcx = 0, dcy = 0;
@@ -125,12 +179,13 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, uint32_t w, T p
   int st = 0;
   if (A::abs(dx1) > T(1.5) || A::abs(dy1) > T(1.5)) st |= 1;
   if (!(gama < T(3.0e38))) st |= 2;  // NaN or overflow
-  // vz for jz: plain uses uz*cva/gama (pic2d.f90:1028); mixed keeps uz/gama
-  // and applies cva when the fixed-point sum is converted.
-  const T vz = MIXED ? A::div(uz, gama) : A::div(A::mul(uz, a.cva), gama);
   const T msp = sp ? a.ms[1] : a.ms[0];
-  o.ke = MIXED ? (double)A::mul(A::div(usq, A::add(gama, one)), msp)
-               : (double)A::mul(A::sub(gama, one), msp);
+  if constexpr (MIXED) {  // (gamma - 1) = u^2 / (gamma + 1) avoids the cancellation of gamma - 1 in FP32
+    const T usq = A::mad(uz, uz, A::mad(uy, uy, A::mul(ux, ux)));
+    o.ke = (double)A::mul(push_fdiv(usq, A::add(gama, one)), msp);
+  } else {
+    o.ke = (double)A::mul(A::sub(gama, one), msp);  // pic2d.f90:1062
+  }
 
   // ---- charge-conserving deposit terms (pic2d.f90:1237-1295), indices
   // relative to the old cell: i1 = j1 = 0, i2 = dcx, j2 = dcy.
@@ -203,8 +258,6 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, uint32_t w, T p
   o.ux = ux;
   o.uy = ruy;
   o.uz = uz;
-  o.ix = ix;
-  o.iy = iy;
   o.dcx = dcx;
   o.dcy = dcy;
   o.di = di;
@@ -231,6 +284,21 @@ __device__ __forceinline__ void term_node(int k, int dcx, int dcy, int di, int d
     case 13: *x = 1; *y = 0; break;
     case 14: *x = 0; *y = 1; break;
     default: *x = 1; *y = 1; break;
+  }
+}
+
+// Component and relative node of entry k of the 17-value cell stencil:
+// 0-1 jx (0,0),(0,1); 2-3 jy (0,0),(1,0); 4-12 jz (x,y) in [-1,1]^2 at
+// 4 + (x+1)*3 + (y+1); 13-16 rho (0,0),(1,0),(0,1),(1,1).
+__device__ __forceinline__ void stencil_node(int k, int* c, int* x, int* y) {
+  if (k < 2) {
+    *c = JX; *x = 0; *y = k;
+  } else if (k < 4) {
+    *c = JY; *x = k - 2; *y = 0;
+  } else if (k < 13) {
+    *c = JZ; *x = (k - 4) / 3 - 1; *y = (k - 4) % 3 - 1;
+  } else {
+    *c = RHO; *x = (k - 13) & 1; *y = (k - 13) >> 1;
   }
 }
 
@@ -262,6 +330,19 @@ __device__ __forceinline__ bool map_current(int c, int gx, int gy, int mx, int m
   return true;
 }
 
+// Bin of cell (cx, cy) in the window of the tile (ixt, rows y0..y1-1): the
+// 3 x (y1-y0+2) cells adjacent to the tile, bin = bx*(tile_rows+2) + by.
+// Returns -1 outside the window.
+__device__ __forceinline__ int window_bin(int cx, int cy, int ixt, int y0, int y1, int ty, int mx, int my,
+                                          int ybc) {
+  int bx = cx - ixt + 1;
+  bx = bx < 0 ? bx + mx : (bx >= mx ? bx - mx : bx);
+  int by = cy - y0 + 1;
+  if (ybc == 0) by = by < 0 ? by + my : (by >= my ? by - my : by);
+  if (bx < 0 || bx > 2 || by < 0 || by > y1 - y0 + 1) return -1;
+  return bx * (ty + 2) + by;
+}
+
 __device__ __forceinline__ void acc_add(double* p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void acc_add(long long* p, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
@@ -276,42 +357,122 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
   }
 }
 
-template <class T, bool MIXED>
-__global__ void __launch_bounds__(NTHREADS) k_push(PushParams<T> a) {
+template <class T>
+struct PushSmem {
+  T stage[NTHREADS / 32][17][33];  // per-warp transposition of the stencil sums
+  double red[32];
+};
+
+// Dynamic shared memory: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
+template <class T, bool MIXED, bool HIST>
+__global__ void __launch_bounds__(NTHREADS, MIXED ? 2 : 1) k_push(PushParams<T> a) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Acc* win = reinterpret_cast<Acc*>(smem_raw);  // [4 comps][4 cols][WR rows]
-  __shared__ double red[32];
-  const int TY = a.tile_rows, WR = TY + 3;
+  __shared__ PushSmem<T> sm;
+  const int TY = a.tile_rows, WR = TY + 3, NB = 3 * (TY + 2);
+  Acc* win = reinterpret_cast<Acc*>(smem_raw);
+  int* hist = reinterpret_cast<int*>(win + 16 * WR);
   const int t = blockIdx.x;
   const int ixt = t / a.tiles_per_col;
   const int y0 = (t - ixt * a.tiles_per_col) * TY;
   const int y1 = min(y0 + TY, a.my);
   for (int e = threadIdx.x; e < 16 * WR; e += blockDim.x) win[e] = Acc(0);
+  if (HIST)
+    for (int e = threadIdx.x; e < NB; e += blockDim.x) hist[e] = 0;
   __syncthreads();
   Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
   const unsigned lane = lane_id();
+  const int w = threadIdx.x >> 5;
+  // this lane's entry of the stencil when it deposits a run's sum
+  int sc = 0, sx = 0, sy = 0;
+  stencil_node(lane < 17 ? (int)lane : 0, &sc, &sx, &sy);
   double ke_e = 0.0, ke_i = 0.0;
   int status = 0;
-  for (int base = pbeg; base < pend; base += NTHREADS) {
-    const int p = base + (int)threadIdx.x;
-    int key = -1 - (int)lane;  // unique negative: never merges, never deposits
-    T v[17];
+  for (int q0 = pbeg & ~(PPT - 1); q0 < pend; q0 += PPT * NTHREADS) {
+    const int q = q0 + PPT * (int)threadIdx.x;
+    uint32_t cw[PPT];
+    T px[PPT], py[PPT], pux[PPT], puy[PPT], puz[PPT];
+    bool act[PPT];
+    const bool full = q >= pbeg && q + PPT <= pend;
+    if (full) {
+      ld4(a.cell + q, cw);
+      ld4(a.dx + q, px);
+      ld4(a.dy + q, py);
+      ld4(a.ux + q, pux);
+      ld4(a.uy + q, puy);
+      ld4(a.uz + q, puz);
 #pragma unroll
-    for (int k = 0; k < 17; ++k) v[k] = T(0);
-    if (p < pend) {
+      for (int j = 0; j < PPT; ++j) act[j] = true;
+    } else {
+#pragma unroll
+      for (int j = 0; j < PPT; ++j) {
+        const int p = q + j;
+        act[j] = p >= pbeg && p < pend;
+        cw[j] = act[j] ? a.cell[p] : 0u;
+        px[j] = act[j] ? a.dx[p] : T(0);
+        py[j] = act[j] ? a.dy[p] : T(0);
+        pux[j] = act[j] ? a.ux[p] : T(0);
+        puy[j] = act[j] ? a.uy[p] : T(0);
+        puz[j] = act[j] ? a.uz[p] : T(0);
+      }
+    }
+    // thread-level accumulation of the stencils of particles sharing a cell
+    T acc[17];
+#pragma unroll
+    for (int k = 0; k < 17; ++k) acc[k] = T(0);
+    int acc_key = -1;
+    int cache_cell = -1;
+    Node6<T> n00{}, n01{}, n10{}, n11{};
+    int bins[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+      bins[j] = -1;
+      if (!act[j]) continue;
+      const uint32_t wrd = cw[j];
+      const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
+      const int cid = (ix << 16) | iy;
+      if (cid != cache_cell) {
+        const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
+        const T* g10 = g00 + (long long)(a.my + 1) * 8;
+        n00 = load_node(g00);
+        n01 = load_node(g00 + 8);
+        n10 = load_node(g10);
+        n11 = load_node(g10 + 8);
+        cache_cell = cid;
+      }
       Pushed<T> o;
-      push_one<T, MIXED>(a, a.cell[p], a.dx[p], a.dy[p], a.ux[p], a.uy[p], a.uz[p], o);
-      const bool inwin = o.ix == ixt && o.iy >= y0 && o.iy < y1;
-      if (inwin && o.dcx == 0 && o.dcy == 0) {
-        key = o.iy - y0;
-        v[0] = o.e[0] + o.e[2];  // jx (0,0)
-        v[1] = o.e[1] + o.e[3];  // jx (0,1)
-        v[2] = o.e[4] + o.e[6];  // jy (0,0)
-        v[3] = o.e[5] + o.e[7];  // jy (1,0)
-        // jz on the 3x3 block around the cell: index 4 + (x+1)*3 + (y+1);
-        // (0,0) <- e8, (di,0) <- e9, (0,dj) <- e10, (di,dj) <- e11, di, dj = +-1
+      push_one<T, MIXED>(a, sp, ix, iy, px[j], py[j], pux[j], puy[j], puz[j], n00, n01, n10, n11, o);
+      status |= o.status;
+      const bool inwin = ix == ixt && iy >= y0 && iy < y1;
+      const bool cross = o.dcx != 0 || o.dcy != 0;
+      if (HIST) {
+        int b = window_bin(cw_ix(o.cw), cw_iy(o.cw), ixt, y0, y1, TY, a.mx, a.my, a.ybc);
+        if (b < 0) {  // only a corrupt offset can jump two cells: keep the particle in its cell
+          status |= 1;
+          o.cw = wrd;
+          b = window_bin(ix, iy, ixt, y0, y1, TY, a.mx, a.my, a.ybc);
+        }
+        bins[j] = b;
+      }
+      if (inwin) {
+        const int key = iy - y0;
+        if (key != acc_key) {
+          if (acc_key >= 0) {  // flush the previous cell's sum (rare: cell change inside a thread)
+#pragma unroll
+            for (int k = 0; k < 17; ++k) {
+              int c, x, y;
+              stencil_node(k, &c, &x, &y);
+              if (acc[k] != T(0)) acc_add(&win[(c * 4 + 1 + x) * WR + acc_key + 1 + y], to_acc<T, MIXED>(acc[k]));
+              acc[k] = T(0);
+            }
+          }
+          acc_key = key;
+        }
+        acc[0] += cross ? o.e[0] : o.e[0] + o.e[2];
+        acc[1] += cross ? o.e[1] : o.e[1] + o.e[3];
+        acc[2] += cross ? o.e[4] : o.e[4] + o.e[6];
+        acc[3] += cross ? o.e[5] : o.e[5] + o.e[7];
 #pragma unroll
         for (int xx = -1; xx <= 1; ++xx)
 #pragma unroll
@@ -321,20 +482,18 @@ __global__ void __launch_bounds__(NTHREADS) k_push(PushParams<T> a) {
             if (xx != 0 && yy == 0 && xx == o.di) z = o.e[9];
             if (xx == 0 && yy != 0 && yy == o.dj) z = o.e[10];
             if (xx != 0 && yy != 0 && xx == o.di && yy == o.dj) z = o.e[11];
-            v[4 + (xx + 1) * 3 + (yy + 1)] = z;
+            acc[4 + (xx + 1) * 3 + (yy + 1)] += z;
           }
-        v[13] = o.e[12];
-        v[14] = o.e[13];
-        v[15] = o.e[14];
-        v[16] = o.e[15];
-      } else if (inwin) {
-        const int wy0 = o.iy - y0 + 1;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          int rx, ry;
-          term_node(k, o.dcx, o.dcy, o.di, o.dj, &rx, &ry);
-          const int c = k >> 2;
-          acc_add(&win[(c * 4 + 1 + rx) * WR + wy0 + ry], to_acc<T, MIXED>(o.e[k]));
+        acc[13] += o.e[12];
+        acc[14] += o.e[13];
+        acc[15] += o.e[14];
+        acc[16] += o.e[15];
+        if (cross) {  // second zig-zag segment, attached to the new cell
+          const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
+          acc_add(&win[(JX * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[2]));
+          acc_add(&win[(JX * 4 + wx) * WR + wy + 1], to_acc<T, MIXED>(o.e[3]));
+          acc_add(&win[(JY * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[6]));
+          acc_add(&win[(JY * 4 + wx + 1) * WR + wy], to_acc<T, MIXED>(o.e[7]));
         }
       } else {
         status |= 4;
@@ -342,46 +501,69 @@ __global__ void __launch_bounds__(NTHREADS) k_push(PushParams<T> a) {
         for (int k = 0; k < 16; ++k) {
           int rx, ry;
           term_node(k, o.dcx, o.dcy, o.di, o.dj, &rx, &ry);
-          const int c = k >> 2;
           long long gi;
           int sg;
-          if (map_current(c, o.ix + rx, o.iy + ry, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
+          if (map_current(k >> 2, ix + rx, iy + ry, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
             acc_add(&gacc[gi], to_acc<T, MIXED>(sg < 0 ? -o.e[k] : o.e[k]));
         }
       }
-      a.cell[p] = o.cw;
-      a.dx[p] = o.dx;
-      a.dy[p] = o.dy;
-      a.ux[p] = o.ux;
-      a.uy[p] = o.uy;
-      a.uz[p] = o.uz;
-      if (cw_sp(o.cw)) ke_e += o.ke;
+      cw[j] = o.cw;
+      px[j] = o.dx;
+      py[j] = o.dy;
+      pux[j] = o.ux;
+      puy[j] = o.uy;
+      puz[j] = o.uz;
+      if (sp) ke_e += o.ke;
       else ke_i += o.ke;
-      status |= o.status;
     }
-    // Sum the stencils of lanes that share a cell; the last lane of each run deposits.
+    if (full) {
+      st4(a.cell + q, cw);
+      st4(a.dx + q, px);
+      st4(a.dy + q, py);
+      st4(a.ux + q, pux);
+      st4(a.uy + q, puy);
+      st4(a.uz + q, puz);
+    } else {
+#pragma unroll
+      for (int j = 0; j < PPT; ++j)
+        if (act[j]) {
+          const int p = q + j;
+          a.cell[p] = cw[j];
+          a.dx[p] = px[j];
+          a.dy[p] = py[j];
+          a.ux[p] = pux[j];
+          a.uy[p] = puy[j];
+          a.uz[p] = puz[j];
+        }
+    }
+    if (HIST) {  // warp-aggregated count of the new cells
+#pragma unroll
+      for (int j = 0; j < PPT; ++j) {
+        const unsigned peers = __match_any_sync(FULL, bins[j]);
+        if (bins[j] >= 0 && (peers & lanemask_lt()) == 0) atomicAdd(&hist[bins[j]], __popc(peers));
+      }
+    }
+    // Sum the stencils of lanes that share a cell; 17 lanes add each run's sum.
+    const int key = acc_key >= 0 ? acc_key : -1 - (int)lane;
     const int kprev = __shfl_up_sync(FULL, key, 1);
     const unsigned head = (lane == 0) || (kprev != key);
-    warp_segmented_scan<T, 17>(v, head);
+    warp_segmented_scan<T, 17>(acc, head);
     const unsigned head_next = __shfl_down_sync(FULL, head, 1);
-    if (key >= 0 && (lane == 31 || head_next)) {
-      const int wy = key + 1;
-      acc_add(&win[(0 * 4 + 1) * WR + wy], to_acc<T, MIXED>(v[0]));
-      acc_add(&win[(0 * 4 + 1) * WR + wy + 1], to_acc<T, MIXED>(v[1]));
-      acc_add(&win[(1 * 4 + 1) * WR + wy], to_acc<T, MIXED>(v[2]));
-      acc_add(&win[(1 * 4 + 2) * WR + wy], to_acc<T, MIXED>(v[3]));
+    const bool tail = acc_key >= 0 && (lane == 31 || head_next);
 #pragma unroll
-      for (int xx = 0; xx < 3; ++xx)
-#pragma unroll
-        for (int yy = 0; yy < 3; ++yy) {
-          const T z = v[4 + xx * 3 + yy];
-          if (z != T(0)) acc_add(&win[(2 * 4 + xx) * WR + wy - 1 + yy], to_acc<T, MIXED>(z));
-        }
-      acc_add(&win[(3 * 4 + 1) * WR + wy], to_acc<T, MIXED>(v[13]));
-      acc_add(&win[(3 * 4 + 2) * WR + wy], to_acc<T, MIXED>(v[14]));
-      acc_add(&win[(3 * 4 + 1) * WR + wy + 1], to_acc<T, MIXED>(v[15]));
-      acc_add(&win[(3 * 4 + 2) * WR + wy + 1], to_acc<T, MIXED>(v[16]));
+    for (int k = 0; k < 17; ++k) sm.stage[w][k][lane] = acc[k];
+    __syncwarp();
+    unsigned tails = __ballot_sync(FULL, tail);
+    while (tails) {
+      const int src = __ffs(tails) - 1;
+      tails &= tails - 1;
+      const int kt = __shfl_sync(FULL, key, src);
+      if (lane < 17) {
+        const T v = sm.stage[w][lane][src];
+        if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+      }
     }
+    __syncwarp();
   }
   __syncthreads();
   // Fold the window into the global current.
@@ -396,8 +578,10 @@ __global__ void __launch_bounds__(NTHREADS) k_push(PushParams<T> a) {
     if (map_current(c, ixt - 1 + wx, y0 - 1 + wy, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
       acc_add(&gacc[gi], sg < 0 ? -val : val);
   }
-  const double se = block_sum(ke_e, red);
-  const double si = block_sum(ke_i, red);
+  if (HIST)
+    for (int e = threadIdx.x; e < NB; e += blockDim.x) a.tilecnt[(long long)t * NB + e] = hist[e];
+  const double se = block_sum(ke_e, sm.red);
+  const double si = block_sum(ke_i, sm.red);
   if (threadIdx.x == 0) {
     a.ke_part[2 * t] = se;
     a.ke_part[2 * t + 1] = si;

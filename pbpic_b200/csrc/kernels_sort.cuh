@@ -14,6 +14,7 @@
 //   3. a gather of every particle array through that permutation.
 #pragma once
 #include "device_common.cuh"
+#include "kernels_push.cuh"
 
 namespace pbd {
 
@@ -219,6 +220,183 @@ __global__ void k_tile_off(const int32_t* off, int ntiles, int tpc, int ty, int 
 __global__ void k_tile_off_uniform(int ntiles, int64_t n, int32_t* tile_off) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t <= ntiles) tile_off[t] = (int32_t)(n * t / ntiles);
+}
+
+}  // namespace pbd
+
+namespace pbd {
+
+// ------------------------------------------------------- fused counting sort
+// When the particles were sorted by cell before the push, a particle of tile T
+// (a run of cells of one column) lands in T's window: the cells adjacent to T.
+// The push counts the new cells per (tile, window bin); with those counts the
+// stable counting sort needs no radix passes:
+//   count(cell) = sum over the tiles whose window holds the cell,
+//   slot(particle) = offset(cell) + [particles of earlier tiles in the cell]
+//                  + [earlier particles of its own tile in the cell],
+// where "earlier" is array order, i.e. tile order then position in the tile.
+
+// Tiles whose window contains cell (cx, cy): the owners of its 3x3 neighbours.
+__device__ __forceinline__ int tiles_of_cell(int cx, int cy, int mx, int my, int ybc, int ty, int tpc, int* tl) {
+  int n = 0;
+#pragma unroll
+  for (int a = -1; a <= 1; ++a) {
+    int x = cx + a;
+    x = x < 0 ? x + mx : (x >= mx ? x - mx : x);
+#pragma unroll
+    for (int b = -1; b <= 1; ++b) {
+      int y = cy + b;
+      if (ybc == 0) {
+        y = y < 0 ? y + my : (y >= my ? y - my : y);
+      } else if (y < 0 || y >= my) {
+        continue;
+      }
+      const int tt = x * tpc + y / ty;
+      bool dup = false;
+      for (int k = 0; k < n; ++k) dup |= tl[k] == tt;
+      if (!dup) tl[n++] = tt;
+    }
+  }
+  return n;
+}
+
+__device__ __forceinline__ int bin_in_tile(int cx, int cy, int tt, int mx, int my, int ybc, int ty, int tpc) {
+  const int ixt = tt / tpc, y0 = (tt - ixt * tpc) * ty, y1 = min(y0 + ty, my);
+  return window_bin(cx, cy, ixt, y0, y1, ty, mx, my, ybc);
+}
+
+struct FusedSortParams {
+  int mx, my, ybc, ty, tpc, ntiles, nb;
+  const int32_t* tilecnt;  // [ntiles][nb] from the push
+  int32_t* counts;         // [mx*my + 1] per-cell counts (last entry 0)
+  const int32_t* off;      // exclusive scan of counts
+  int32_t* base;           // [ntiles][nb] first slot of each (tile, bin)
+};
+
+__global__ void k_fused_counts(FusedSortParams a) {
+  const int64_t ncells = (int64_t)a.mx * a.my;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
+    if (c == ncells) {
+      a.counts[c] = 0;
+      continue;
+    }
+    const int cx = (int)(c / a.my), cy = (int)(c - (int64_t)cx * a.my);
+    int tl[9];
+    const int n = tiles_of_cell(cx, cy, a.mx, a.my, a.ybc, a.ty, a.tpc, tl);
+    int32_t s = 0;
+    for (int k = 0; k < n; ++k) {
+      const int b = bin_in_tile(cx, cy, tl[k], a.mx, a.my, a.ybc, a.ty, a.tpc);
+      if (b >= 0) s += a.tilecnt[(int64_t)tl[k] * a.nb + b];
+    }
+    a.counts[c] = s;
+  }
+}
+
+__global__ void k_fused_base(FusedSortParams a) {
+  const int64_t n = (int64_t)a.ntiles * a.nb;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int tt = (int)(e / a.nb), b = (int)(e - (int64_t)tt * a.nb);
+    int32_t base = 0;
+    if (a.tilecnt[e] > 0) {
+      const int ixt = tt / a.tpc, y0 = (tt - ixt * a.tpc) * a.ty;
+      const int bx = b / (a.ty + 2), by = b - bx * (a.ty + 2);
+      int cx = ixt - 1 + bx;
+      cx = cx < 0 ? cx + a.mx : (cx >= a.mx ? cx - a.mx : cx);
+      int cy = y0 - 1 + by;
+      if (a.ybc == 0) cy = cy < 0 ? cy + a.my : (cy >= a.my ? cy - a.my : cy);
+      const int64_t c = (int64_t)cx * a.my + cy;
+      base = a.off[c];
+      int tl[9];
+      const int nt = tiles_of_cell(cx, cy, a.mx, a.my, a.ybc, a.ty, a.tpc, tl);
+      for (int k = 0; k < nt; ++k) {
+        if (tl[k] >= tt) continue;
+        const int b2 = bin_in_tile(cx, cy, tl[k], a.mx, a.my, a.ybc, a.ty, a.tpc);
+        if (b2 >= 0) base += a.tilecnt[(int64_t)tl[k] * a.nb + b2];
+      }
+    }
+    a.base[e] = base;
+  }
+}
+
+template <class T>
+struct ScatterParams {
+  int mx, my, ybc, ty, tpc, nb;
+  const int32_t* tile_off;  // position ranges of the tiles (those the push used)
+  const int32_t* base;      // [ntiles][nb]
+  const uint32_t* ci;
+  const T *dxi, *dyi, *uxi, *uyi, *uzi;
+  const int32_t* pidi;
+  uint32_t* co;
+  T *dxo, *dyo, *uxo, *uyo, *uzo;
+  int32_t* pido;
+};
+
+constexpr int SC_IPT = 8, SC_CHUNK = 256 * SC_IPT, SC_MAXNB = 3 * (64 + 2) + 1;
+
+// Stable scatter of one tile. Warp w owns the chunk range [w*256, (w+1)*256),
+// item k of lane l at k*32 + l, so (warp, item, lane) order is array order.
+template <class T>
+__global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
+  __shared__ int32_t cnt[8][SC_MAXNB];
+  __shared__ int32_t run[SC_MAXNB], sbase[SC_MAXNB];
+  const int t = blockIdx.x;
+  const int ixt = t / a.tpc, y0 = (t - ixt * a.tpc) * a.ty, y1 = min(y0 + a.ty, a.my);
+  const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = lane_id(), lt = lanemask_lt();
+  for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
+    run[b] = 0;
+    sbase[b] = a.base[(int64_t)t * a.nb + b];
+  }
+  for (int c0 = pbeg; c0 < pend; c0 += SC_CHUNK) {
+    for (int e = threadIdx.x; e < 8 * SC_MAXNB; e += blockDim.x) (&cnt[0][0])[e] = 0;
+    __syncthreads();
+    int bin[SC_IPT], pos[SC_IPT];
+#pragma unroll
+    for (int k = 0; k < SC_IPT; ++k) {
+      const int p = c0 + w * 256 + k * 32 + (int)lane;
+      int b = a.nb;  // sentinel: beyond the tile
+      if (p < pend) {
+        const uint32_t cw = a.ci[p];
+        b = window_bin(cw_ix(cw), cw_iy(cw), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
+        if (b < 0) b = a.nb;  // cannot happen: the push kept every particle in its window
+      }
+      const unsigned peers = __match_any_sync(FULL, b);
+      const int before = cnt[w][b];
+      __syncwarp();
+      if ((peers & lt) == 0) cnt[w][b] = before + __popc(peers);
+      __syncwarp();
+      pos[k] = before + __popc(peers & lt);
+      bin[k] = b;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
+      int32_t r = run[b];
+#pragma unroll
+      for (int ww = 0; ww < 8; ++ww) {
+        const int32_t c = cnt[ww][b];
+        cnt[ww][b] = r;
+        r += c;
+      }
+      run[b] = r;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SC_IPT; ++k) {
+      const int p = c0 + w * 256 + k * 32 + (int)lane;
+      if (p < pend && bin[k] < a.nb) {
+        const int64_t d = (int64_t)sbase[bin[k]] + cnt[w][bin[k]] + pos[k];
+        a.co[d] = a.ci[p];
+        a.dxo[d] = a.dxi[p];
+        a.dyo[d] = a.dyi[p];
+        a.uxo[d] = a.uxi[p];
+        a.uyo[d] = a.uyi[p];
+        a.uzo[d] = a.uzi[p];
+        if (a.pido) a.pido[d] = a.pidi[p];
+      }
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace pbd

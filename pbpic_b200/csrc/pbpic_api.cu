@@ -149,6 +149,11 @@ struct pbpic_handle {
   int32_t* rhist = nullptr;
   int32_t* scan_scratch = nullptr;
   bool sorted = false;
+  bool fused_ok = false;    // grid admits the fused counting sort (distinct window cells)
+  bool hist_valid = false;  // the last push counted new cells per tile on a sorted array
+  int nb = 0;               // window bins per tile, 3*(TY+2)
+  int32_t* tilecnt = nullptr;
+  int32_t* tbase = nullptr;
   void* staging = nullptr;
   size_t staging_bytes = 0;
   double* rho = nullptr;
@@ -236,6 +241,7 @@ PushParams<T> push_params(pbpic_handle* h) {
   p.uz = P<T>(h, b, 4);
   p.ng = (const T*)h->ng;
   p.jacc = h->jacc;
+  p.tilecnt = h->tilecnt;
   const T dt = (T)c.dt, mime = (T)c.mime, cva = (T)c.cva, dx = (T)c.dx, dy = (T)c.dy;
   for (int s = 0; s < 2; ++s) {
     const T q = s == 0 ? T(1) : T(-1);
@@ -322,11 +328,16 @@ int set_unsorted_tiles(pbpic_handle* h) {
   k_tile_off_uniform<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, h->stream>>>(h->ntiles, h->n, h->tile_off);
   CKLAUNCH("k_tile_off_uniform");
   h->sorted = false;
+  h->hist_valid = false;
   return PBPIC_OK;
 }
 
 template <class T, bool MIXED>
+int do_fused_sort(pbpic_handle* h);
+
+template <class T, bool MIXED>
 int do_sort(pbpic_handle* h) {
+  if (h->hist_valid) return do_fused_sort<T, MIXED>(h);
   cudaStream_t s = h->stream;
   const int64_t n = h->n;
   CK(cudaMemsetAsync(h->counts, 0, (size_t)(h->ncells + 1) * 4, s));
@@ -352,6 +363,7 @@ int do_sort(pbpic_handle* h) {
                                                                   (int32_t)n, h->tile_off);
   CKLAUNCH("k_tile_off");
   h->sorted = true;
+  h->hist_valid = false;
   return PBPIC_OK;
 }
 
@@ -361,12 +373,75 @@ int do_push(pbpic_handle* h) {
   TRY(ensure_hist(h, h->itime + 2));
   CK(cudaMemsetAsync(h->jacc, 0, (size_t)4 * plane_elems(h) * 8, s));
   PushParams<T> p = push_params<T, MIXED>(h);
-  const size_t smem = (size_t)16 * (h->TY + 3) * 8;
-  k_push<T, MIXED><<<h->ntiles, NTHREADS, smem, s>>>(p);
+  const size_t smem = (size_t)16 * (h->TY + 3) * 8 + (size_t)h->nb * 4;
+  const bool hist = h->sorted && h->fused_ok;
+  if (hist) k_push<T, MIXED, true><<<h->ntiles, NTHREADS, smem, s>>>(p);
+  else k_push<T, MIXED, false><<<h->ntiles, NTHREADS, smem, s>>>(p);
   CKLAUNCH("k_push");
   k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
   CKLAUNCH("k_energy_row");
+  h->hist_valid = hist;
   h->sorted = false;
+  return PBPIC_OK;
+}
+
+// Counting sort from the per-tile histograms of the last push (kernels_sort.cuh).
+template <class T, bool MIXED>
+int do_fused_sort(pbpic_handle* h) {
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  FusedSortParams f;
+  f.mx = h->cfg.mx;
+  f.my = h->cfg.my;
+  f.ybc = h->cfg.ybc;
+  f.ty = h->TY;
+  f.tpc = h->tpc;
+  f.ntiles = h->ntiles;
+  f.nb = h->nb;
+  f.tilecnt = h->tilecnt;
+  f.counts = h->counts;
+  f.off = h->off;
+  f.base = h->tbase;
+  k_fused_counts<<<grid_for((int64_t)h->ncells + 1, 256), 256, 0, s>>>(f);
+  CKLAUNCH("k_fused_counts");
+  CK(cudaMemcpyAsync(h->off, h->counts, (size_t)(h->ncells + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  TRY(scan_excl(s, h->off, h->ncells + 1, h->scan_scratch));
+  k_fused_base<<<grid_for((int64_t)h->ntiles * h->nb, 256), 256, 0, s>>>(f);
+  CKLAUNCH("k_fused_base");
+  const int b = h->cur, o = 1 - b;
+  ScatterParams<T> sp;
+  sp.mx = f.mx;
+  sp.my = f.my;
+  sp.ybc = f.ybc;
+  sp.ty = f.ty;
+  sp.tpc = f.tpc;
+  sp.nb = f.nb;
+  sp.tile_off = h->tile_off;
+  sp.base = h->tbase;
+  sp.ci = h->cell[b];
+  sp.dxi = P<T>(h, b, 0);
+  sp.dyi = P<T>(h, b, 1);
+  sp.uxi = P<T>(h, b, 2);
+  sp.uyi = P<T>(h, b, 3);
+  sp.uzi = P<T>(h, b, 4);
+  sp.pidi = h->pid[b];
+  sp.co = h->cell[o];
+  sp.dxo = P<T>(h, o, 0);
+  sp.dyo = P<T>(h, o, 1);
+  sp.uxo = P<T>(h, o, 2);
+  sp.uyo = P<T>(h, o, 3);
+  sp.uzo = P<T>(h, o, 4);
+  sp.pido = h->pid[o];
+  if (n > 0) {
+    k_fused_scatter<T><<<h->ntiles, 256, 0, s>>>(sp);
+    CKLAUNCH("k_fused_scatter");
+    h->cur = o;
+  }
+  k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, h->cfg.my,
+                                                                  (int32_t)n, h->tile_off);
+  CKLAUNCH("k_tile_off");
+  h->sorted = true;
+  h->hist_valid = false;
   return PBPIC_OK;
 }
 
@@ -654,9 +729,18 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
   h->tsz = h->mixed ? 4 : 8;
   h->S = c.my + 1;
   h->ncells = c.mx * c.my;
-  h->TY = c.tile_rows > 0 ? std::min(c.tile_rows, c.my) : std::min(c.my, 32);
+  if (c.tile_rows < 0 || c.tile_rows > 64) {
+    delete h;
+    return fail(PBPIC_EINVAL, "tile_rows must be in [0, 64]");
+  }
+  // Default tile: 32 rows; with periodic y at most my-2 rows, so that a tile's
+  // window (the adjacent cells) holds distinct cells and the fused sort applies.
+  const int ty_default = c.ybc == PBPIC_BC_PERIODIC ? std::max(1, std::min(32, c.my - 2)) : std::min(32, c.my);
+  h->TY = c.tile_rows > 0 ? std::min(c.tile_rows, c.my) : ty_default;
   h->tpc = (c.my + h->TY - 1) / h->TY;
   h->ntiles = c.mx * h->tpc;
+  h->nb = 3 * (h->TY + 2);
+  h->fused_ok = c.mx >= 3 && (c.ybc == PBPIC_BC_CONDUCTING || c.my >= h->TY + 2);
   h->cap = c.capacity;
   const size_t capn = (size_t)std::max<int64_t>(c.capacity, 1);
   const int64_t pe = plane_elems(h);
@@ -677,6 +761,8 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
   A(&h->counts, (size_t)(h->ncells + 1) * 4);
   A(&h->off, (size_t)(h->ncells + 1) * 4);
   A(&h->tile_off, (size_t)(h->ntiles + 1) * 4);
+  A(&h->tilecnt, (size_t)h->ntiles * h->nb * 4);
+  A(&h->tbase, (size_t)h->ntiles * h->nb * 4);
   A(&h->ke_part, (size_t)std::max(h->ntiles, 148 * 16) * 2 * 8);
   h->nke = 148 * 8;
   h->nfe = grid_for((int64_t)(c.mx + 1) * (c.my + 1), 256, 148 * 8);

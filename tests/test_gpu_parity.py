@@ -275,3 +275,30 @@ def test_bad_particle_records_are_rejected(gpu_lib, oracle_mod):
             s.load_particles(p)
         with pytest.raises(pbpic_b200.PbpicError):
             s.load_particles(np.concatenate([p, p]))  # over capacity
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("ybc,mx,my,ty", [(0, 16, 12, 0), (0, 9, 20, 6), (1, 16, 12, 0), (1, 7, 13, 5), (1, 8, 40, 64)])
+def test_fused_sort_is_the_stable_sort(gpu_lib, oracle_mod, precision, ybc, mx, my, ty):
+    """After a push on a sorted array, the counting sort from the push's
+    per-tile histograms gives exactly the stable sort by cell (array order
+    within a cell) of the pushed particles, and the per-cell counts."""
+    cfg, ld, p, _ = plasma(oracle_mod, ybc, mx=mx, my=my, ppc=6, vthe=0.6)
+    yee = random_fields(cfg, 5, amp=0.2)
+    with new_sim(cfg, len(p), precision=precision, tile_rows=ty) as s:
+        s.load_particles(p)
+        s.load_fields(yee)
+        s.countingsort()
+        for _ in range(3):
+            s.pusher()
+            pre = s.particles()
+            s.fieldsolver()
+            s.countingsort()
+            post = s.particles()
+            order = np.argsort(pre["grid"], kind="stable")
+            assert np.array_equal(post["pid"], pre["pid"][order])
+            assert np.array_equal(post["grid"], pre["grid"][order])
+            for c in COMPS:
+                assert np.array_equal(post[c], pre[c][order])
+            assert np.array_equal(s.cell_counts(), np.bincount(pre["grid"] - 1, minlength=mx * my))
+        assert s.status() == 0
