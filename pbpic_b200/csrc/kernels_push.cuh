@@ -5,10 +5,10 @@
 //
 // Work decomposition: a tile is a run of `tile_rows` cells of one column
 // (contiguous in the cell-sorted order); one block pushes the particles of one
-// tile. Each thread takes 4 consecutive particles per pass, read and written
-// with 128-bit accesses. Consecutive particles of a sorted array share their
-// cell, so a thread keeps the 4 gather nodes of its current cell in registers
-// and sums the deposit stencils of its particles before touching memory.
+// tile. Each thread takes 8 consecutive particles per pass, read and written
+// in groups of 4 with 128-bit accesses. Consecutive particles of a sorted
+// array share their cell, so a thread sums the deposit stencils of its
+// particles in registers before touching memory.
 //
 // Deposit: the zig-zag move of a particle splits at the relay point into a
 // segment in the old cell and one in the new cell. Everything attached to the
@@ -30,8 +30,6 @@
 #include "device_common.cuh"
 
 namespace pbd {
-
-constexpr int PPT = 4;  // particles per thread per pass
 
 template <class T>
 struct PushParams {
@@ -101,7 +99,7 @@ struct Pushed {
   T dx, dy, ux, uy, uz;  // new state (after reflection)
   int dcx, dcy, di, dj;  // cell steps and jz quadrant
   T e[16];               // deposit terms: jx 4, jy 4, jz 4, rho 4
-  double ke;
+  T ke;                  // kinetic energy (gamma - 1) ms
   int status;
 };
 
@@ -166,50 +164,72 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
   // move, pic2d.f90:1005-1023
   const T dx1 = A::mad(A::mul(c3, ux), a.idx, px);
   const T dy1 = A::mad(A::mul(c3, uy), a.idy, py);
-  int dcx = 0, dcy = 0;
-  T dx2 = dx1, dy2 = dy1;
-  if (A::abs(dx1) > half) {
-    dcx = dx1 >= T(0) ? 1 : -1;
-    dx2 = A::add(dx1, dx1 >= T(0) ? -one : one);
-  }
-  if (A::abs(dy1) > half) {
-    dcy = dy1 >= T(0) ? 1 : -1;
-    dy2 = A::add(dy1, dy1 >= T(0) ? -one : one);
-  }
+  // cell steps (pic2d.f90:1008-1023), also as floating-point values for the deposit
+  const T fdcx = dx1 > half ? one : (dx1 < -half ? -one : T(0));
+  const T fdcy = dy1 > half ? one : (dy1 < -half ? -one : T(0));
+  const int dcx = dx1 > half ? 1 : (dx1 < -half ? -1 : 0);
+  const int dcy = dy1 > half ? 1 : (dy1 < -half ? -1 : 0);
+  const T dx2 = A::sub(dx1, fdcx);
+  const T dy2 = A::sub(dy1, fdcy);
   int st = 0;
   if (A::abs(dx1) > T(1.5) || A::abs(dy1) > T(1.5)) st |= 1;
   if (!(gama < T(3.0e38))) st |= 2;  // NaN or overflow
   const T msp = sp ? a.ms[1] : a.ms[0];
   if constexpr (MIXED) {  // (gamma - 1) = u^2 / (gamma + 1) avoids the cancellation of gamma - 1 in FP32
     const T usq = A::mad(uz, uz, A::mad(uy, uy, A::mul(ux, ux)));
-    o.ke = (double)A::mul(push_fdiv(usq, A::add(gama, one)), msp);
+    o.ke = A::mul(push_fdiv(usq, A::add(gama, one)), msp);
   } else {
-    o.ke = (double)A::mul(A::sub(gama, one), msp);  // pic2d.f90:1062
+    o.ke = A::mul(A::sub(gama, one), msp);  // pic2d.f90:1062
   }
 
   // ---- charge-conserving deposit terms (pic2d.f90:1237-1295), indices
   // relative to the old cell: i1 = j1 = 0, i2 = dcx, j2 = dcy.
   const T qx = sp ? a.qx[1] : a.qx[0], qy = sp ? a.qy[1] : a.qy[0], qq = sp ? a.q[1] : a.q[0];
-  const T im = A::mul(A::add(A::add(A::add(T(dcx), px), dx2), one), half);
-  const T jm = A::mul(A::add(A::add(A::add(T(dcy), py), dy2), one), half);
-  const T ir = fmin(T(dcx < 0 ? dcx : 0) + one, fmax(T(dcx > 0 ? dcx : 0), im));
-  const T jr = fmin(T(dcy < 0 ? dcy : 0) + one, fmax(T(dcy > 0 ? dcy : 0), jm));
-  const T fx1 = A::mul(qx, A::sub(A::sub(ir, px), half));
-  const T fy1 = A::mul(qy, A::sub(A::sub(jr, py), half));
-  const T fx2 = A::mul(qx, A::sub(A::add(A::add(T(dcx), dx2), half), ir));
-  const T fy2 = A::mul(qy, A::sub(A::add(A::add(T(dcy), dy2), half), jr));
-  const T wx1 = A::mul(A::add(A::add(ir, px), half), half);
-  const T wy1 = A::mul(A::add(A::add(jr, py), half), half);
-  const T wx2 = A::mul(A::add(A::add(A::sub(ir, T(dcx)), dx2), half), half);
-  const T wy2 = A::mul(A::add(A::add(A::sub(jr, T(dcy)), dy2), half), half);
-  o.e[0] = A::mul(fx1, A::sub(one, wy1));  // jx (0, 0)
-  o.e[1] = A::mul(fx1, wy1);               // jx (0, 1)
-  o.e[2] = A::mul(fx2, A::sub(one, wy2));  // jx (dcx, dcy)
-  o.e[3] = A::mul(fx2, wy2);               // jx (dcx, dcy+1)
-  o.e[4] = A::mul(fy1, A::sub(one, wx1));  // jy (0, 0)
-  o.e[5] = A::mul(fy1, wx1);               // jy (1, 0)
-  o.e[6] = A::mul(fy2, A::sub(one, wx2));  // jy (dcx, dcy)
-  o.e[7] = A::mul(fy2, wx2);               // jy (dcx+1, dcy)
+  T im, jm;
+  if constexpr (MIXED) {
+    // Positions in cell units from the old cell's lower-left node: start
+    // xs = dx0 + 1/2, end xe = dx1 + 1/2 (= dcx + dx2 + 1/2). The relay point
+    // is the midpoint for a particle that stays, else the face it crosses.
+    const T xs = A::add(px, half), xe = A::add(dx1, half);
+    const T ys = A::add(py, half), ye = A::add(dy1, half);
+    im = A::mul(A::add(xs, xe), half);
+    jm = A::mul(A::add(ys, ye), half);
+    const T ir = dcx == 0 ? im : (dcx > 0 ? one : T(0));
+    const T jr = dcy == 0 ? jm : (dcy > 0 ? one : T(0));
+    const T fx1 = A::mul(qx, A::sub(ir, xs)), fx2 = A::mul(qx, A::sub(xe, ir));
+    const T fy1 = A::mul(qy, A::sub(jr, ys)), fy2 = A::mul(qy, A::sub(ye, jr));
+    const T wx1 = A::mul(A::add(ir, xs), half), wy1 = A::mul(A::add(jr, ys), half);
+    const T wx2 = A::sub(A::mul(A::add(ir, xe), half), fdcx), wy2 = A::sub(A::mul(A::add(jr, ye), half), fdcy);
+    o.e[0] = A::mad(-fx1, wy1, fx1);  // jx (0, 0)
+    o.e[1] = A::mul(fx1, wy1);        // jx (0, 1)
+    o.e[2] = A::mad(-fx2, wy2, fx2);  // jx (dcx, dcy)
+    o.e[3] = A::mul(fx2, wy2);        // jx (dcx, dcy+1)
+    o.e[4] = A::mad(-fy1, wx1, fy1);  // jy (0, 0)
+    o.e[5] = A::mul(fy1, wx1);        // jy (1, 0)
+    o.e[6] = A::mad(-fy2, wx2, fy2);  // jy (dcx, dcy)
+    o.e[7] = A::mul(fy2, wx2);        // jy (dcx+1, dcy)
+  } else {
+    im = A::mul(A::add(A::add(A::add(fdcx, px), dx2), one), half);
+    jm = A::mul(A::add(A::add(A::add(fdcy, py), dy2), one), half);
+    const T ir = fmin(fmin(fdcx, T(0)) + one, fmax(fmax(fdcx, T(0)), im));
+    const T jr = fmin(fmin(fdcy, T(0)) + one, fmax(fmax(fdcy, T(0)), jm));
+    const T fx1 = A::mul(qx, A::sub(A::sub(ir, px), half));
+    const T fy1 = A::mul(qy, A::sub(A::sub(jr, py), half));
+    const T fx2 = A::mul(qx, A::sub(A::add(A::add(fdcx, dx2), half), ir));
+    const T fy2 = A::mul(qy, A::sub(A::add(A::add(fdcy, dy2), half), jr));
+    const T wx1 = A::mul(A::add(A::add(ir, px), half), half);
+    const T wy1 = A::mul(A::add(A::add(jr, py), half), half);
+    const T wx2 = A::mul(A::add(A::add(A::sub(ir, fdcx), dx2), half), half);
+    const T wy2 = A::mul(A::add(A::add(A::sub(jr, fdcy), dy2), half), half);
+    o.e[0] = A::mul(fx1, A::sub(one, wy1));  // jx (0, 0)
+    o.e[1] = A::mul(fx1, wy1);               // jx (0, 1)
+    o.e[2] = A::mul(fx2, A::sub(one, wy2));  // jx (dcx, dcy)
+    o.e[3] = A::mul(fx2, wy2);               // jx (dcx, dcy+1)
+    o.e[4] = A::mul(fy1, A::sub(one, wx1));  // jy (0, 0)
+    o.e[5] = A::mul(fy1, wx1);               // jy (1, 0)
+    o.e[6] = A::mul(fy2, A::sub(one, wx2));  // jy (dcx, dcy)
+    o.e[7] = A::mul(fy2, wx2);               // jy (dcx+1, dcy)
+  }
   T dimid = A::sub(im, half), djmid = A::sub(jm, half);
   const int di = dimid >= T(0) ? 1 : -1, dj = djmid >= T(0) ? 1 : -1;
   dimid = A::abs(dimid);
@@ -357,16 +377,77 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
   }
 }
 
+// Compile-time shape of the push loop: particles per thread per pass are
+// 4 * PBPIC_PUSH_HALVES (read as float4 groups), and PBPIC_PUSH_UNROLL selects
+// whether the loop over the 4 particles of a group is unrolled.
+#ifndef PBPIC_PUSH_HALVES
+#define PBPIC_PUSH_HALVES 2
+#endif
+#ifndef PBPIC_PUSH_UNROLL
+#define PBPIC_PUSH_UNROLL 0
+#endif
+#ifndef PBPIC_PUSH_MINBLOCKS
+#define PBPIC_PUSH_MINBLOCKS 2
+#endif
+#ifndef PBPIC_PUSH_NODECACHE
+#define PBPIC_PUSH_NODECACHE 0
+#endif
+
 template <class T>
 struct PushSmem {
   T stage[NTHREADS / 32][17][33];  // per-warp transposition of the stencil sums
   double red[32];
 };
 
+// Rare path: a particle outside its tile adds its 16 terms (staged in the
+// thread's shared-memory column, stride 33) to global memory.
+template <class T, bool MIXED>
+__device__ __noinline__ void deposit_global(const PushParams<T>& a, const T* col, int ix, int iy, int dcx, int dcy,
+                                            int di, int dj) {
+  using Acc = typename std::conditional<MIXED, long long, double>::type;
+  Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
+  for (int k = 0; k < 16; ++k) {
+    int rx, ry;
+    term_node(k, dcx, dcy, di, dj, &rx, &ry);
+    long long gi;
+    int sg;
+    const T v = col[k * 33];
+    if (map_current(k >> 2, ix + rx, iy + ry, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
+      acc_add(&gacc[gi], to_acc<T, MIXED>(sg < 0 ? -v : v));
+  }
+}
+
+// Rare path: a thread's particles changed cell inside a pass; add the finished
+// cell's stencil (staged in shared memory, stride 33) to the window.
+template <class T, bool MIXED>
+__device__ __noinline__ void flush_column(typename std::conditional<MIXED, long long, double>::type* win,
+                                          const T* col, int key, int WR) {
+  for (int k = 0; k < 17; ++k) {
+    int c, x, y;
+    stencil_node(k, &c, &x, &y);
+    const T v = col[k * 33];
+    if (v != T(0)) acc_add(&win[(c * 4 + 1 + x) * WR + key + 1 + y], to_acc<T, MIXED>(v));
+  }
+}
+
+template <class V>
+__device__ __forceinline__ V pick4(const V (&v)[4], int j) {
+  return j == 0 ? v[0] : (j == 1 ? v[1] : (j == 2 ? v[2] : v[3]));
+}
+template <class V>
+__device__ __forceinline__ void put4(V (&v)[4], int j, V x) {
+  v[0] = j == 0 ? x : v[0];
+  v[1] = j == 1 ? x : v[1];
+  v[2] = j == 2 ? x : v[2];
+  v[3] = j == 3 ? x : v[3];
+}
+
 // Dynamic shared memory: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
 template <class T, bool MIXED, bool HIST>
-__global__ void __launch_bounds__(NTHREADS, MIXED ? 2 : 1) k_push(PushParams<T> a) {
+__global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
+  constexpr int G = PBPIC_PUSH_HALVES;  // float4 groups per thread per pass
+  constexpr int PT = 4 * G;             // particles per thread per pass
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T> sm;
   const int TY = a.tile_rows, WR = TY + 3, NB = 3 * (TY + 2);
@@ -387,36 +468,10 @@ __global__ void __launch_bounds__(NTHREADS, MIXED ? 2 : 1) k_push(PushParams<T> 
   // this lane's entry of the stencil when it deposits a run's sum
   int sc = 0, sx = 0, sy = 0;
   stencil_node(lane < 17 ? (int)lane : 0, &sc, &sx, &sy);
+  T* mycol = &sm.stage[w][0][lane];
   double ke_e = 0.0, ke_i = 0.0;
   int status = 0;
-  for (int q0 = pbeg & ~(PPT - 1); q0 < pend; q0 += PPT * NTHREADS) {
-    const int q = q0 + PPT * (int)threadIdx.x;
-    uint32_t cw[PPT];
-    T px[PPT], py[PPT], pux[PPT], puy[PPT], puz[PPT];
-    bool act[PPT];
-    const bool full = q >= pbeg && q + PPT <= pend;
-    if (full) {
-      ld4(a.cell + q, cw);
-      ld4(a.dx + q, px);
-      ld4(a.dy + q, py);
-      ld4(a.ux + q, pux);
-      ld4(a.uy + q, puy);
-      ld4(a.uz + q, puz);
-#pragma unroll
-      for (int j = 0; j < PPT; ++j) act[j] = true;
-    } else {
-#pragma unroll
-      for (int j = 0; j < PPT; ++j) {
-        const int p = q + j;
-        act[j] = p >= pbeg && p < pend;
-        cw[j] = act[j] ? a.cell[p] : 0u;
-        px[j] = act[j] ? a.dx[p] : T(0);
-        py[j] = act[j] ? a.dy[p] : T(0);
-        pux[j] = act[j] ? a.ux[p] : T(0);
-        puy[j] = act[j] ? a.uy[p] : T(0);
-        puz[j] = act[j] ? a.uz[p] : T(0);
-      }
-    }
+  for (int q0 = pbeg & ~3; q0 < pend; q0 += PT * NTHREADS) {
     // thread-level accumulation of the stencils of particles sharing a cell
     T acc[17];
 #pragma unroll
@@ -424,125 +479,167 @@ __global__ void __launch_bounds__(NTHREADS, MIXED ? 2 : 1) k_push(PushParams<T> 
     int acc_key = -1;
     int cache_cell = -1;
     Node6<T> n00{}, n01{}, n10{}, n11{};
-    int bins[PPT];
+    T pke_e = T(0), pke_i = T(0);  // this pass's kinetic energy, per species
+#pragma unroll 1
+    for (int g = 0; g < G; ++g) {
+      const int q = q0 + PT * (int)threadIdx.x + 4 * g;
+      uint32_t cw[4];
+      T px[4], py[4], pux[4], puy[4], puz[4];
+      const bool full = q >= pbeg && q + 4 <= pend;
+      if (full) {
+        ld4(a.cell + q, cw);
+        ld4(a.dx + q, px);
+        ld4(a.dy + q, py);
+        ld4(a.ux + q, pux);
+        ld4(a.uy + q, puy);
+        ld4(a.uz + q, puz);
+      } else {
 #pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-      bins[j] = -1;
-      if (!act[j]) continue;
-      const uint32_t wrd = cw[j];
-      const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
-      const int cid = (ix << 16) | iy;
-      if (cid != cache_cell) {
-        const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
-        const T* g10 = g00 + (long long)(a.my + 1) * 8;
-        n00 = load_node(g00);
-        n01 = load_node(g00 + 8);
-        n10 = load_node(g10);
-        n11 = load_node(g10 + 8);
-        cache_cell = cid;
-      }
-      Pushed<T> o;
-      push_one<T, MIXED>(a, sp, ix, iy, px[j], py[j], pux[j], puy[j], puz[j], n00, n01, n10, n11, o);
-      status |= o.status;
-      const bool inwin = ix == ixt && iy >= y0 && iy < y1;
-      const bool cross = o.dcx != 0 || o.dcy != 0;
-      if (HIST) {
-        int b = window_bin(cw_ix(o.cw), cw_iy(o.cw), ixt, y0, y1, TY, a.mx, a.my, a.ybc);
-        if (b < 0) {  // only a corrupt offset can jump two cells: keep the particle in its cell
-          status |= 1;
-          o.cw = wrd;
-          b = window_bin(ix, iy, ixt, y0, y1, TY, a.mx, a.my, a.ybc);
+        for (int j = 0; j < 4; ++j) {
+          const int p = q + j;
+          const bool act = p >= pbeg && p < pend;
+          cw[j] = act ? a.cell[p] : 0u;
+          px[j] = act ? a.dx[p] : T(0);
+          py[j] = act ? a.dy[p] : T(0);
+          pux[j] = act ? a.ux[p] : T(0);
+          puy[j] = act ? a.uy[p] : T(0);
+          puz[j] = act ? a.uz[p] : T(0);
         }
-        bins[j] = b;
       }
-      if (inwin) {
-        const int key = iy - y0;
-        if (key != acc_key) {
-          if (acc_key >= 0) {  // flush the previous cell's sum (rare: cell change inside a thread)
+      int bins[4] = {-1, -1, -1, -1};
+#if PBPIC_PUSH_UNROLL
 #pragma unroll
-            for (int k = 0; k < 17; ++k) {
-              int c, x, y;
-              stencil_node(k, &c, &x, &y);
-              if (acc[k] != T(0)) acc_add(&win[(c * 4 + 1 + x) * WR + acc_key + 1 + y], to_acc<T, MIXED>(acc[k]));
-              acc[k] = T(0);
+#else
+#pragma unroll 1
+#endif
+      for (int j = 0; j < 4; ++j) {
+        const int p = q + j;
+        if (p < pbeg || p >= pend) continue;
+        const uint32_t wrd = pick4(cw, j);
+        const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
+        const int cid = (ix << 16) | iy;
+        if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
+          const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
+          const T* g10 = g00 + (long long)(a.my + 1) * 8;
+          n00 = load_node(g00);
+          n01 = load_node(g00 + 8);
+          n10 = load_node(g10);
+          n11 = load_node(g10 + 8);
+          cache_cell = cid;
+        }
+        Pushed<T> o;
+        push_one<T, MIXED>(a, sp, ix, iy, pick4(px, j), pick4(py, j), pick4(pux, j), pick4(puy, j),
+                           pick4(puz, j), n00, n01, n10, n11, o);
+        status |= o.status;
+        const bool inwin = ix == ixt && iy >= y0 && iy < y1;
+        const bool cross = o.dcx != 0 || o.dcy != 0;
+        if (HIST) {
+          // new cell in the tile's window: column 1 + dcx, row new_iy - y0 + 1
+          // (wrapped rows come back through +-my; a reflected particle keeps its row)
+          int by = cw_iy(o.cw) - y0 + 1;
+          by = by < 0 ? by + a.my : (by > y1 - y0 + 1 ? by - a.my : by);
+          int b = (1 + o.dcx) * (TY + 2) + by;
+          if (!inwin || by < 0 || by > y1 - y0 + 1) {
+            b = window_bin(cw_ix(o.cw), cw_iy(o.cw), ixt, y0, y1, TY, a.mx, a.my, a.ybc);
+            if (b < 0) {  // only a corrupt offset can jump two cells: keep the particle in its cell
+              status |= 1;
+              o.cw = wrd;
+              b = window_bin(ix, iy, ixt, y0, y1, TY, a.mx, a.my, a.ybc);
             }
           }
-          acc_key = key;
+          put4(bins, j, b);
         }
-        acc[0] += cross ? o.e[0] : o.e[0] + o.e[2];
-        acc[1] += cross ? o.e[1] : o.e[1] + o.e[3];
-        acc[2] += cross ? o.e[4] : o.e[4] + o.e[6];
-        acc[3] += cross ? o.e[5] : o.e[5] + o.e[7];
+        if (inwin) {
+          const int key = iy - y0;
+          if (key != acc_key) {
+            if (acc_key >= 0) {  // rare: the thread's particles changed cell
 #pragma unroll
-        for (int xx = -1; xx <= 1; ++xx)
-#pragma unroll
-          for (int yy = -1; yy <= 1; ++yy) {
-            T z = T(0);
-            if (xx == 0 && yy == 0) z = o.e[8];
-            if (xx != 0 && yy == 0 && xx == o.di) z = o.e[9];
-            if (xx == 0 && yy != 0 && yy == o.dj) z = o.e[10];
-            if (xx != 0 && yy != 0 && xx == o.di && yy == o.dj) z = o.e[11];
-            acc[4 + (xx + 1) * 3 + (yy + 1)] += z;
+              for (int k = 0; k < 17; ++k) {
+                mycol[k * 33] = acc[k];
+                acc[k] = T(0);
+              }
+              flush_column<T, MIXED>(win, mycol, acc_key, WR);
+            }
+            acc_key = key;
           }
-        acc[13] += o.e[12];
-        acc[14] += o.e[13];
-        acc[15] += o.e[14];
-        acc[16] += o.e[15];
-        if (cross) {  // second zig-zag segment, attached to the new cell
-          const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
-          acc_add(&win[(JX * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[2]));
-          acc_add(&win[(JX * 4 + wx) * WR + wy + 1], to_acc<T, MIXED>(o.e[3]));
-          acc_add(&win[(JY * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[6]));
-          acc_add(&win[(JY * 4 + wx + 1) * WR + wy], to_acc<T, MIXED>(o.e[7]));
+          acc[0] += cross ? o.e[0] : o.e[0] + o.e[2];
+          acc[1] += cross ? o.e[1] : o.e[1] + o.e[3];
+          acc[2] += cross ? o.e[4] : o.e[4] + o.e[6];
+          acc[3] += cross ? o.e[5] : o.e[5] + o.e[7];
+          // jz: (0,0) <- e8, (di,0) <- e9, (0,dj) <- e10, (di,dj) <- e11 with di, dj = +-1
+          const T zxm = o.di < 0 ? T(1) : T(0), zxp = o.di > 0 ? T(1) : T(0);
+          const T zym = o.dj < 0 ? T(1) : T(0), zyp = o.dj > 0 ? T(1) : T(0);
+          acc[4 + 0] += zxm * zym * o.e[11];
+          acc[4 + 1] += zxm * o.e[9];
+          acc[4 + 2] += zxm * zyp * o.e[11];
+          acc[4 + 3] += zym * o.e[10];
+          acc[4 + 4] += o.e[8];
+          acc[4 + 5] += zyp * o.e[10];
+          acc[4 + 6] += zxp * zym * o.e[11];
+          acc[4 + 7] += zxp * o.e[9];
+          acc[4 + 8] += zxp * zyp * o.e[11];
+          acc[13] += o.e[12];
+          acc[14] += o.e[13];
+          acc[15] += o.e[14];
+          acc[16] += o.e[15];
+          if (cross) {  // second zig-zag segment, attached to the new cell
+            const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
+            acc_add(&win[(JX * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[2]));
+            acc_add(&win[(JX * 4 + wx) * WR + wy + 1], to_acc<T, MIXED>(o.e[3]));
+            acc_add(&win[(JY * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[6]));
+            acc_add(&win[(JY * 4 + wx + 1) * WR + wy], to_acc<T, MIXED>(o.e[7]));
+          }
+        } else {
+          status |= 4;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) mycol[k * 33] = o.e[k];
+          deposit_global<T, MIXED>(a, mycol, ix, iy, o.dcx, o.dcy, o.di, o.dj);
         }
+        put4(cw, j, o.cw);
+        put4(px, j, o.dx);
+        put4(py, j, o.dy);
+        put4(pux, j, o.ux);
+        put4(puy, j, o.uy);
+        put4(puz, j, o.uz);
+        if (sp) pke_e += o.ke;
+        else pke_i += o.ke;
+      }
+      if (full) {
+        st4(a.cell + q, cw);
+        st4(a.dx + q, px);
+        st4(a.dy + q, py);
+        st4(a.ux + q, pux);
+        st4(a.uy + q, puy);
+        st4(a.uz + q, puz);
       } else {
-        status |= 4;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          int rx, ry;
-          term_node(k, o.dcx, o.dcy, o.di, o.dj, &rx, &ry);
-          long long gi;
-          int sg;
-          if (map_current(k >> 2, ix + rx, iy + ry, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
-            acc_add(&gacc[gi], to_acc<T, MIXED>(sg < 0 ? -o.e[k] : o.e[k]));
-        }
-      }
-      cw[j] = o.cw;
-      px[j] = o.dx;
-      py[j] = o.dy;
-      pux[j] = o.ux;
-      puy[j] = o.uy;
-      puz[j] = o.uz;
-      if (sp) ke_e += o.ke;
-      else ke_i += o.ke;
-    }
-    if (full) {
-      st4(a.cell + q, cw);
-      st4(a.dx + q, px);
-      st4(a.dy + q, py);
-      st4(a.ux + q, pux);
-      st4(a.uy + q, puy);
-      st4(a.uz + q, puz);
-    } else {
-#pragma unroll
-      for (int j = 0; j < PPT; ++j)
-        if (act[j]) {
+        for (int j = 0; j < 4; ++j) {
           const int p = q + j;
-          a.cell[p] = cw[j];
-          a.dx[p] = px[j];
-          a.dy[p] = py[j];
-          a.ux[p] = pux[j];
-          a.uy[p] = puy[j];
-          a.uz[p] = puz[j];
+          if (p >= pbeg && p < pend) {
+            a.cell[p] = cw[j];
+            a.dx[p] = px[j];
+            a.dy[p] = py[j];
+            a.ux[p] = pux[j];
+            a.uy[p] = puy[j];
+            a.uz[p] = puz[j];
+          }
         }
-    }
-    if (HIST) {  // warp-aggregated count of the new cells
+      }
+      if (HIST) {  // warp-aggregated count of the new cells
 #pragma unroll
-      for (int j = 0; j < PPT; ++j) {
-        const unsigned peers = __match_any_sync(FULL, bins[j]);
-        if (bins[j] >= 0 && (peers & lanemask_lt()) == 0) atomicAdd(&hist[bins[j]], __popc(peers));
+        for (int j = 0; j < 4; ++j) {
+          const int b0 = __shfl_sync(FULL, bins[j], 0);
+          if (__all_sync(FULL, bins[j] == b0)) {  // common: the whole warp lands in one cell
+            if (lane == 0 && b0 >= 0) atomicAdd(&hist[b0], 32);
+          } else {
+            const unsigned peers = __match_any_sync(FULL, bins[j]);
+            if (bins[j] >= 0 && (peers & lanemask_lt()) == 0) atomicAdd(&hist[bins[j]], __popc(peers));
+          }
+        }
       }
     }
+    ke_e += (double)pke_e;
+    ke_i += (double)pke_i;
     // Sum the stencils of lanes that share a cell; 17 lanes add each run's sum.
     const int key = acc_key >= 0 ? acc_key : -1 - (int)lane;
     const int kprev = __shfl_up_sync(FULL, key, 1);
@@ -550,8 +647,9 @@ __global__ void __launch_bounds__(NTHREADS, MIXED ? 2 : 1) k_push(PushParams<T> 
     warp_segmented_scan<T, 17>(acc, head);
     const unsigned head_next = __shfl_down_sync(FULL, head, 1);
     const bool tail = acc_key >= 0 && (lane == 31 || head_next);
+    __syncwarp();
 #pragma unroll
-    for (int k = 0; k < 17; ++k) sm.stage[w][k][lane] = acc[k];
+    for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
     __syncwarp();
     unsigned tails = __ballot_sync(FULL, tail);
     while (tails) {

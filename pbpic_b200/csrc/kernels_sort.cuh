@@ -331,10 +331,15 @@ struct ScatterParams {
   int32_t* pido;
 };
 
-constexpr int SC_IPT = 8, SC_CHUNK = 256 * SC_IPT, SC_MAXNB = 3 * (64 + 2) + 1;
+#ifndef PBPIC_SCATTER_IPT
+#define PBPIC_SCATTER_IPT 8
+#endif
+constexpr int SC_IPT = PBPIC_SCATTER_IPT, SC_CHUNK = 256 * SC_IPT, SC_MAXNB = 3 * (64 + 2) + 1;
 
-// Stable scatter of one tile. Warp w owns the chunk range [w*256, (w+1)*256),
-// item k of lane l at k*32 + l, so (warp, item, lane) order is array order.
+// Stable scatter of one tile. Warp w owns the chunk range
+// [w*32*SC_IPT, (w+1)*32*SC_IPT), item k of lane l at k*32 + l, so
+// (warp, item, lane) order is array order. All loads of a chunk are issued
+// before the ranking so that they overlap.
 template <class T>
 __global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
   __shared__ int32_t cnt[8][SC_MAXNB];
@@ -352,13 +357,28 @@ __global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
     for (int e = threadIdx.x; e < 8 * SC_MAXNB; e += blockDim.x) (&cnt[0][0])[e] = 0;
     __syncthreads();
     int bin[SC_IPT], pos[SC_IPT];
+    uint32_t vc[SC_IPT];
+    T vdx[SC_IPT], vdy[SC_IPT], vux[SC_IPT], vuy[SC_IPT], vuz[SC_IPT];
+    int32_t vpid[SC_IPT];
+    // issue every load of the chunk before ranking (memory-level parallelism)
 #pragma unroll
     for (int k = 0; k < SC_IPT; ++k) {
-      const int p = c0 + w * 256 + k * 32 + (int)lane;
+      const int p = c0 + w * (32 * SC_IPT) + k * 32 + (int)lane;
+      const bool ok = p < pend;
+      vc[k] = ok ? a.ci[p] : 0u;
+      vdx[k] = ok ? a.dxi[p] : T(0);
+      vdy[k] = ok ? a.dyi[p] : T(0);
+      vux[k] = ok ? a.uxi[p] : T(0);
+      vuy[k] = ok ? a.uyi[p] : T(0);
+      vuz[k] = ok ? a.uzi[p] : T(0);
+      vpid[k] = (ok && a.pidi) ? a.pidi[p] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < SC_IPT; ++k) {
+      const int p = c0 + w * (32 * SC_IPT) + k * 32 + (int)lane;
       int b = a.nb;  // sentinel: beyond the tile
       if (p < pend) {
-        const uint32_t cw = a.ci[p];
-        b = window_bin(cw_ix(cw), cw_iy(cw), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
+        b = window_bin(cw_ix(vc[k]), cw_iy(vc[k]), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
         if (b < 0) b = a.nb;  // cannot happen: the push kept every particle in its window
       }
       const unsigned peers = __match_any_sync(FULL, b);
@@ -383,16 +403,15 @@ __global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < SC_IPT; ++k) {
-      const int p = c0 + w * 256 + k * 32 + (int)lane;
-      if (p < pend && bin[k] < a.nb) {
+      if (bin[k] < a.nb) {
         const int64_t d = (int64_t)sbase[bin[k]] + cnt[w][bin[k]] + pos[k];
-        a.co[d] = a.ci[p];
-        a.dxo[d] = a.dxi[p];
-        a.dyo[d] = a.dyi[p];
-        a.uxo[d] = a.uxi[p];
-        a.uyo[d] = a.uyi[p];
-        a.uzo[d] = a.uzi[p];
-        if (a.pido) a.pido[d] = a.pidi[p];
+        a.co[d] = vc[k];
+        a.dxo[d] = vdx[k];
+        a.dyo[d] = vdy[k];
+        a.uxo[d] = vux[k];
+        a.uyo[d] = vuy[k];
+        a.uzo[d] = vuz[k];
+        if (a.pido) a.pido[d] = vpid[k];
       }
     }
     __syncthreads();

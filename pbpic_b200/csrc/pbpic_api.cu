@@ -733,9 +733,9 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
     delete h;
     return fail(PBPIC_EINVAL, "tile_rows must be in [0, 64]");
   }
-  // Default tile: 32 rows; with periodic y at most my-2 rows, so that a tile's
+  // Default tile: 64 rows; with periodic y at most my-2 rows, so that a tile's
   // window (the adjacent cells) holds distinct cells and the fused sort applies.
-  const int ty_default = c.ybc == PBPIC_BC_PERIODIC ? std::max(1, std::min(32, c.my - 2)) : std::min(32, c.my);
+  const int ty_default = c.ybc == PBPIC_BC_PERIODIC ? std::max(1, std::min(64, c.my - 2)) : std::min(64, c.my);
   h->TY = c.tile_rows > 0 ? std::min(c.tile_rows, c.my) : ty_default;
   h->tpc = (c.my + h->TY - 1) / h->TY;
   h->ntiles = c.mx * h->tpc;
