@@ -199,6 +199,20 @@ int pbpic_kernel_launches(int64_t* count);
 int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
                              int32_t* perm_dev, int32_t* counts_dev, void* stream);
 
+/* The same stable counting sort with no device allocation at all, for callers
+ * that cannot call cudaMalloc: host code whose GPU memory is already owned by
+ * another allocator (a framework's caching allocator that reserved the device),
+ * or a time loop that must not pay for the synchronisation an allocation
+ * implies. It has no counterpart in the reference. Its scratch is a static
+ * device array inside the library, sized for PBPIC_STATIC_SORT_MAX_KEYS keys
+ * (about 17 MB, held on every GPU that loads the library until the process
+ * exits); larger n is rejected with PBPIC_ECAPACITY. The first call on a device
+ * looks up the array's address and should come before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race. */
+#define PBPIC_STATIC_SORT_MAX_KEYS 1048576
+int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t ncells,
+                                    int32_t* perm_dev, int32_t* counts_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

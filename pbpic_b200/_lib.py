@@ -90,7 +90,10 @@ SIGNATURES = {
     "pbpic_status": [_P, _PI32],
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],
     "pbpic_kernel_launches": [_PI64],
+    "pbpic_counting_sort_keys_static": [_P, _I64, _I32, _P, _P, _P],
 }
+
+STATIC_SORT_MAX_KEYS = 1048576  # PBPIC_STATIC_SORT_MAX_KEYS
 
 _lib = None
 

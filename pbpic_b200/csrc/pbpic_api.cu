@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1066,3 +1067,87 @@ int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
 }
 
 }  // extern "C"
+
+// ============================================================================
+// pbpic_counting_sort_keys_static: the stateless counting sort without any
+// device allocation, for callers that cannot call cudaMalloc: a host code whose
+// device memory is owned up front by another allocator (for example a
+// framework's caching allocator that has reserved the GPU), or a time loop that
+// must not trigger the device-wide synchronisation of an allocation.
+//
+// Its scratch is the file-scope array below, sized for
+// PBPIC_STATIC_SORT_MAX_KEYS keys. Every GPU that loads this library holds the
+// array until the process exits. Host code cannot use the array's name as a
+// device address, so the first call on each device (with that device current)
+// looks the address up with cudaGetSymbolAddress and keeps it; make that first
+// call before any stream capture. All calls share the array and it keeps the
+// last call's contents: the only word that must start at zero (the key-range
+// status) is cleared on every call, and calls that overlap on the GPU (on
+// different streams or host threads) race on the array.
+// ============================================================================
+namespace {
+
+constexpr int64_t kStaticKeys = PBPIC_STATIC_SORT_MAX_KEYS;
+constexpr int64_t kStaticHist = 256 * ((kStaticKeys + RTILE - 1) / RTILE);
+constexpr int64_t kStaticScan = 1024;  // chunk totals of every scan level of the histogram (needs 19)
+constexpr int64_t kStaticWords = 4 * kStaticKeys + kStaticHist + kStaticScan + 64;
+
+static __device__ __align__(256) int32_t g_static_sort_scratch[kStaticWords];
+
+std::mutex g_static_mu;
+int32_t* g_static_addr[1024] = {};  // device address of the array, per device ordinal
+
+int static_sort_scratch(int32_t** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 1024) return fail(PBPIC_EINVAL, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_sort_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(PBPIC_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_static_addr[dev] = (int32_t*)p;
+  }
+  *out = g_static_addr[dev];
+  return PBPIC_OK;
+}
+
+}  // namespace
+
+extern "C" int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t ncells,
+                                               int32_t* perm_dev, int32_t* counts_dev, void* stream) {
+  if (n < 0 || ncells <= 0) return fail(PBPIC_EINVAL, "bad n or ncells");
+  if (n > kStaticKeys)
+    return fail(PBPIC_ECAPACITY, "n = " + std::to_string(n) + " exceeds the static scratch limit of " +
+                                     std::to_string(kStaticKeys) + " keys (PBPIC_STATIC_SORT_MAX_KEYS)");
+  if (n > 0 && (!keys_dev || !perm_dev)) return fail(PBPIC_EINVAL, "null device buffer");
+  if (!counts_dev) return fail(PBPIC_EINVAL, "null counts buffer");
+  if (scan_scratch_ints(radix_hist_ints(std::max<int64_t>(n, 1))) > kStaticScan)
+    return fail(PBPIC_EINVAL, "static scan scratch too small");
+  int32_t* base = nullptr;
+  TRY(static_sort_scratch(&base));
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t* k0 = base;
+  int32_t* k1 = k0 + kStaticKeys;
+  int32_t* v0 = k1 + kStaticKeys;
+  int32_t* v1 = v0 + kStaticKeys;
+  int32_t* rhist = v1 + kStaticKeys;
+  int32_t* scr = rhist + kStaticHist;
+  int* status = (int*)(scr + kStaticScan);
+  CK(cudaMemsetAsync(counts_dev, 0, (size_t)ncells * 4, s));
+  CK(cudaMemsetAsync(status, 0, sizeof(int), s));
+  if (n > 0) {
+    k_key_hist<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(keys_dev, n, ncells, counts_dev, status);
+    CKLAUNCH("k_key_hist");
+    CK(cudaMemcpyAsync(k0, keys_dev, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    int32_t* perm = nullptr;
+    TRY(radix_sort(s, n, ncells, k0, k1, v0, v1, rhist, scr, &perm));
+    CK(cudaMemcpyAsync(perm_dev, perm, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  }
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (st & 8) return fail(PBPIC_EINVAL, "key outside [0, ncells)");
+  return PBPIC_OK;
+}
