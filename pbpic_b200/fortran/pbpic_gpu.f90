@@ -1,0 +1,119 @@
+!******************************************************************************
+! pbpic_gpu: Fortran 2003 ISO_C_BINDING interface to the C ABI of the B200
+! step (include/pbpic.h). It lets the reference's time loop
+! (src/programs/pic2d.f90:171-188) call the GPU step in place of its own
+! subroutines:
+!
+!     call pusher        ->  ierr = pbpic_push(h)          (pic2d.f90:177)
+!     call fieldsolver   ->  ierr = pbpic_fieldsolve(h)    (pic2d.f90:178)
+!     call countingsort  ->  ierr = pbpic_sort(h)          (pic2d.f90:161, 181)
+!
+! The reference's `type particle` (pic2d.f90:47-50) has no bind(c) or sequence
+! attribute, so its layout is compiler-defined; c_particle below is the
+! interoperable record (5 x real(c_float), 3 x integer(c_int32_t), 32 bytes)
+! that pbpic_load_particles_f32 / pbpic_store_particles_f32 exchange. Copy
+! ptl(1:nptlact) into an array of c_particle before loading.
+!
+! Not compiled in the build environment of this repository (it has no Fortran
+! compiler); the interfaces follow include/pbpic.h one to one.
+!******************************************************************************
+module pbpic_gpu
+    use iso_c_binding
+    implicit none
+
+    integer(c_int), parameter :: PBPIC_OK = 0
+    integer(c_int32_t), parameter :: PBPIC_BC_PERIODIC = 0, PBPIC_BC_CONDUCTING = 1
+    integer(c_int32_t), parameter :: PBPIC_FP64_PLAIN = 0, PBPIC_FP32_MIXED = 1
+    integer(c_int32_t), parameter :: PBPIC_COMPAT_BORIS = 1, PBPIC_COMPAT_FOLD = 2, PBPIC_COMPAT_RHO = 4
+
+    type, bind(c) :: pbpic_config
+        integer(c_int32_t) :: mx, my
+        real(c_double) :: dx, dy, dt, cva, mime, in0
+        integer(c_int32_t) :: ybc, precision, compat, track_pid
+        integer(c_int64_t) :: capacity
+        integer(c_int32_t) :: tile_rows, reserved
+    end type
+
+    type, bind(c) :: c_particle
+        real(c_float) :: dx, dy, ux, uy, uz
+        integer(c_int32_t) :: grid, q, pid
+    end type
+
+    interface
+        function pbpic_create(cfg, h) bind(c, name="pbpic_create") result(ierr)
+            import :: c_int, c_ptr, pbpic_config
+            type(pbpic_config), intent(in) :: cfg
+            type(c_ptr), intent(out) :: h
+            integer(c_int) :: ierr
+        end function
+        function pbpic_destroy(h) bind(c, name="pbpic_destroy") result(ierr)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int) :: ierr
+        end function
+        function pbpic_load_particles_f32(h, p, n) bind(c, name="pbpic_load_particles_f32") result(ierr)
+            import :: c_int, c_ptr, c_int64_t, c_particle
+            type(c_ptr), value :: h
+            type(c_particle), intent(in) :: p(*)
+            integer(c_int64_t), value :: n
+            integer(c_int) :: ierr
+        end function
+        function pbpic_store_particles_f32(h, p, cap, n) bind(c, name="pbpic_store_particles_f32") result(ierr)
+            import :: c_int, c_ptr, c_int64_t, c_particle
+            type(c_ptr), value :: h
+            type(c_particle), intent(out) :: p(*)
+            integer(c_int64_t), value :: cap
+            integer(c_int64_t), intent(out) :: n
+            integer(c_int) :: ierr
+        end function
+        function pbpic_load_fields_f64(h, yee6) bind(c, name="pbpic_load_fields_f64") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: yee6(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_store_fields_f64(h, yee6) bind(c, name="pbpic_store_fields_f64") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: yee6(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_push(h) bind(c, name="pbpic_push") result(ierr)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int) :: ierr
+        end function
+        function pbpic_fieldsolve(h) bind(c, name="pbpic_fieldsolve") result(ierr)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int) :: ierr
+        end function
+        function pbpic_sort(h) bind(c, name="pbpic_sort") result(ierr)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int) :: ierr
+        end function
+        function pbpic_step(h, nsteps, sort_every) bind(c, name="pbpic_step") result(ierr)
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: nsteps, sort_every
+            integer(c_int) :: ierr
+        end function
+        function pbpic_energies(h, e) bind(c, name="pbpic_energies") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: e(4)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_cell_counts(h, counts) bind(c, name="pbpic_cell_counts") result(ierr)
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), intent(out) :: counts(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_last_error() bind(c, name="pbpic_last_error") result(msg)
+            import :: c_ptr
+            type(c_ptr) :: msg
+        end function
+    end interface
+end module pbpic_gpu
