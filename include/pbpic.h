@@ -213,6 +213,44 @@ int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
 int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t ncells,
                                     int32_t* perm_dev, int32_t* counts_dev, void* stream);
 
+/* ------------------------------------------------------ differentiable form */
+/* Gradients of a time-integrated loss of the GEM Harris sheet with respect to
+ * the perturbation amplitude psi0, the background density nb and T_i/T_e, by
+ * the discrete adjoint of the step (reverse Boris rotation, deposition adjoint
+ * as a gather, field-gather adjoint as a scatter-add, transposed FDTD update),
+ * with the particle state checkpointed every checkpoint_every steps and
+ * recomputed between checkpoints. The particle set is loaded at the nominal
+ * background density nb0; nb enters as the weight nb/nb0 of the background
+ * particles, which makes the loss differentiable in nb. No counterpart in the
+ * reference (which has no gradients). */
+#define PBPIC_LOSS_MAGNETIC 0 /* sum over steps of dt * magnetic field energy */
+
+typedef struct pbpic_diff_config {
+  int32_t mx, my;       /* cells; conducting walls in y, periodic in x */
+  int32_t ppc;          /* macro-particles per cell per species */
+  int32_t precision;    /* PBPIC_FP64_PLAIN or PBPIC_FP32_MIXED (FP32 forward, FP64 loss and adjoint sums) */
+  double dx;            /* cell size (d_i), dy = dx */
+  double mime, wpe_wce; /* mass ratio, omega_pe / omega_ce */
+  double lambda, nb0;   /* sheet half-thickness (d_i), nominal background density */
+  double cfl;           /* c dt sqrt(1/dx^2 + 1/dy^2) */
+  int32_t nsteps, checkpoint_every, loss, reserved;
+  uint64_t seed;
+} pbpic_diff_config;
+
+typedef struct pbpic_diff_params {
+  double psi0;  /* GEM perturbation, B0 d_i */
+  double nb;    /* background density / n0 */
+  double ti_te; /* ion to electron temperature ratio */
+} pbpic_diff_params;
+
+typedef struct pbpic_diff pbpic_diff;
+int pbpic_diff_create(const pbpic_diff_config* cfg, pbpic_diff** out);
+int pbpic_diff_destroy(pbpic_diff* d);
+/* Load the sheet for `params`, run nsteps keeping checkpoints, return the loss. */
+int pbpic_diff_forward(pbpic_diff* d, const pbpic_diff_params* params, double* loss);
+/* d loss / d (psi0, nb, ti_te) at the parameters of the last forward call. */
+int pbpic_diff_backward(pbpic_diff* d, double grad[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,22 @@ class Loader(ctypes.Structure):
     ]
 
 
+class DiffConfig(ctypes.Structure):
+    _fields_ = [
+        ("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("ppc", ctypes.c_int32), ("precision", ctypes.c_int32),
+        ("dx", ctypes.c_double), ("mime", ctypes.c_double), ("wpe_wce", ctypes.c_double),
+        ("lambda_", ctypes.c_double), ("nb0", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("nsteps", ctypes.c_int32), ("checkpoint_every", ctypes.c_int32), ("loss", ctypes.c_int32),
+        ("reserved", ctypes.c_int32), ("seed", ctypes.c_uint64),
+    ]
+
+
+class DiffParams(ctypes.Structure):
+    _fields_ = [("psi0", ctypes.c_double), ("nb", ctypes.c_double), ("ti_te", ctypes.c_double)]
+
+
+LOSS_MAGNETIC = 0
+
 # The reference's `type particle` (pic2d.f90:47-50) and its double-precision twin.
 PARTICLE_F32 = np.dtype([("dx", "<f4"), ("dy", "<f4"), ("ux", "<f4"), ("uy", "<f4"), ("uz", "<f4"),
                          ("grid", "<i4"), ("q", "<i4"), ("pid", "<i4")])
@@ -91,6 +107,10 @@ SIGNATURES = {
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],
     "pbpic_kernel_launches": [_PI64],
     "pbpic_counting_sort_keys_static": [_P, _I64, _I32, _P, _P, _P],
+    "pbpic_diff_create": [ctypes.POINTER(DiffConfig), ctypes.POINTER(_P)],
+    "pbpic_diff_destroy": [_P],
+    "pbpic_diff_forward": [_P, ctypes.POINTER(DiffParams), _PD],
+    "pbpic_diff_backward": [_P, _PD],
 }
 
 STATIC_SORT_MAX_KEYS = 1048576  # PBPIC_STATIC_SORT_MAX_KEYS

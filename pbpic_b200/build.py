@@ -1,7 +1,8 @@
 """Build the CUDA library of the pbpic B200 step in-tree.
 
-`python -m pbpic_b200.build` compiles pbpic_b200/csrc/pbpic_api.cu (which
-includes every kernel) for sm_100a into pbpic_b200/libpbpic.so, and the C++
+`python -m pbpic_b200.build` compiles pbpic_b200/csrc/pbpic_api.cu and
+pbpic_diff.cu (which include the kernels) for sm_100a into
+pbpic_b200/libpbpic.so, and the C++
 host driver (the reference time loop on the C ABI) into
 pbpic_b200/pic2d_driver. Nothing is compiled at import time.
 """
@@ -61,7 +62,8 @@ def build(force=False, verbose=False, ptxas_verbose=False):
         flags = list(NVCC_FLAGS)
         if ptxas_verbose:
             flags += ["-Xptxas", "-v"]
-        _run([nvcc(), *flags, "-shared", "-o", LIB, os.path.join(CSRC, "pbpic_api.cu")], verbose)
+        cus = [os.path.join(CSRC, f) for f in ("pbpic_api.cu", "pbpic_diff.cu")]
+        _run([nvcc(), *flags, "-shared", "-o", LIB, *cus], verbose)
     drv_src = os.path.join(CSRC, "pic2d_driver.cpp")
     if os.path.exists(drv_src) and (force or _stale(DRIVER, src + [LIB])):
         _run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", DRIVER, drv_src,

@@ -180,7 +180,7 @@ __global__ void k_nodes(FieldParams<T> a) {
 // Sum the per-tile kinetic and per-block field partials in a fixed order and
 // write one row (electron KE, ion KE, E energy, B energy) of the history.
 // Either pointer may be null, in which case that half of the row is kept.
-__global__ void k_energy_row(const double* ke_part, int nke, const double* fe_part, int nfe,
+static __global__ void k_energy_row(const double* ke_part, int nke, const double* fe_part, int nfe,
                              double fe_scale, double fb_scale, double* row) {
   __shared__ double red[32];
   double s[4] = {0, 0, 0, 0};

@@ -22,7 +22,7 @@ namespace pbd {
 constexpr int SCAN_BT = 256, SCAN_IPT = 16, SCAN_TILE = SCAN_BT * SCAN_IPT;
 
 // Exclusive scan of each SCAN_TILE chunk in place; chunk totals to sums[].
-__global__ void __launch_bounds__(SCAN_BT) k_scan_local(int32_t* data, int64_t n, int32_t* sums) {
+static __global__ void __launch_bounds__(SCAN_BT) k_scan_local(int32_t* data, int64_t n, int32_t* sums) {
   __shared__ int32_t buf[SCAN_TILE];
   __shared__ int32_t ws[SCAN_BT / 32];
   const int t = threadIdx.x;
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(SCAN_BT) k_scan_local(int32_t* data, int64_t n
   }
 }
 
-__global__ void k_scan_add(int32_t* data, int64_t n, const int32_t* sums) {
+static __global__ void k_scan_add(int32_t* data, int64_t n, const int32_t* sums) {
   const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
   const int32_t add = sums[blockIdx.x];
   for (int k = threadIdx.x; k < SCAN_TILE; k += blockDim.x) {
@@ -84,7 +84,7 @@ __global__ void k_scan_add(int32_t* data, int64_t n, const int32_t* sums) {
 
 // ------------------------------------------------------------ histogram
 // keys[i] = dense cell of particle i (ix*my + iy); counts[key] += 1.
-__global__ void k_cell_keys(const uint32_t* cell, int64_t n, int my, int32_t* keys, int32_t* counts) {
+static __global__ void k_cell_keys(const uint32_t* cell, int64_t n, int my, int32_t* keys, int32_t* counts) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool ok = i < n;
   int key = -1;
@@ -98,7 +98,7 @@ __global__ void k_cell_keys(const uint32_t* cell, int64_t n, int my, int32_t* ke
 }
 
 // Histogram of caller-provided keys, flagging keys outside [0, ncells).
-__global__ void k_key_hist(const int32_t* keys, int64_t n, int32_t ncells, int32_t* counts, int* status) {
+static __global__ void k_key_hist(const int32_t* keys, int64_t n, int32_t ncells, int32_t* counts, int* status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool ok = i < n;
   int key = -1;
@@ -117,7 +117,7 @@ __global__ void k_key_hist(const int32_t* keys, int64_t n, int32_t ncells, int32
 constexpr int RB = 256, RIPT = 16, RTILE = RB * RIPT, RWARPS = RB / 32;
 
 // Per-block histogram of one 8-bit digit, written digit-major: hist[d * nblocks + b].
-__global__ void __launch_bounds__(RB) k_radix_up(const int32_t* keys, int64_t n, int shift,
+static __global__ void __launch_bounds__(RB) k_radix_up(const int32_t* keys, int64_t n, int shift,
                                                  int32_t* hist, int nblocks) {
   __shared__ int32_t h[256];
   const int t = threadIdx.x;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(RB) k_radix_up(const int32_t* keys, int64_t n,
 // Stable scatter of one digit. Warp w owns the contiguous index range
 // [base + w*32*RIPT, base + (w+1)*32*RIPT), item k of lane l at offset k*32 + l,
 // so (warp, item, lane) order is array order.
-__global__ void __launch_bounds__(RB) k_radix_down(const int32_t* kin, const int32_t* vin, int64_t n,
+static __global__ void __launch_bounds__(RB) k_radix_down(const int32_t* kin, const int32_t* vin, int64_t n,
                                                    int shift, const int32_t* hist_off, int nblocks,
                                                    int32_t* kout, int32_t* vout) {
   __shared__ int32_t cnt[RWARPS][257];
@@ -204,7 +204,7 @@ __global__ void k_gather(const int32_t* perm, int64_t n, const uint32_t* ci, con
 }
 
 // Tile ranges from cell offsets: tile t starts at cell (t / tpc)*my + (t % tpc)*ty.
-__global__ void k_tile_off(const int32_t* off, int ntiles, int tpc, int ty, int my, int32_t n,
+static __global__ void k_tile_off(const int32_t* off, int ntiles, int tpc, int ty, int my, int32_t n,
                            int32_t* tile_off) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t > ntiles) return;
@@ -217,7 +217,7 @@ __global__ void k_tile_off(const int32_t* off, int ntiles, int tpc, int ty, int 
 }
 
 // Equal-count partition of positions (particles not sorted by cell).
-__global__ void k_tile_off_uniform(int ntiles, int64_t n, int32_t* tile_off) {
+static __global__ void k_tile_off_uniform(int ntiles, int64_t n, int32_t* tile_off) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t <= ntiles) tile_off[t] = (int32_t)(n * t / ntiles);
 }
@@ -273,7 +273,7 @@ struct FusedSortParams {
   int32_t* base;           // [ntiles][nb] first slot of each (tile, bin)
 };
 
-__global__ void k_fused_counts(FusedSortParams a) {
+static __global__ void k_fused_counts(FusedSortParams a) {
   const int64_t ncells = (int64_t)a.mx * a.my;
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
     if (c == ncells) {
@@ -292,7 +292,7 @@ __global__ void k_fused_counts(FusedSortParams a) {
   }
 }
 
-__global__ void k_fused_base(FusedSortParams a) {
+static __global__ void k_fused_base(FusedSortParams a) {
   const int64_t n = (int64_t)a.ntiles * a.nb;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int tt = (int)(e / a.nb), b = (int)(e - (int64_t)tt * a.nb);

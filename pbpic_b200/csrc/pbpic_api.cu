@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/pbpic.h"
+#include "api_internal.h"
 #include "device_common.cuh"
 #include "kernels_field.cuh"
 #include "kernels_misc.cuh"
@@ -123,6 +124,9 @@ struct DevT {
 };
 
 }  // namespace
+
+int pbpic_internal_fail(int code, const std::string& msg) { return fail(code, msg); }
+void pbpic_internal_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ===================================================================== handle
 struct pbpic_handle {
