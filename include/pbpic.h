@@ -213,6 +213,45 @@ int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
 int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t ncells,
                                     int32_t* perm_dev, int32_t* counts_dev, void* stream);
 
+/* ------------------------------------------------------------ batched form */
+/* Many independent domains of uneven grid size and particle count advanced
+ * together. Every phase of a step runs once for all domains: persistent
+ * blocks over one table of (domain, tile) pairs for the push and the
+ * scatter of the counting sort, one grid row per domain for the rest. The
+ * counting sort runs every step, and pairs of steps are replayed from a
+ * captured CUDA graph on the batch's own stream. Domains are FP32 mixed.
+ * Tile rows (per domain) and particles per thread are set by hand or by
+ * pbpic_batch_autotune. A domain's particles, fields and energies after n
+ * batched steps are bit-identical to pbpic_step(h, n, 1) on a handle with
+ * the same tile rows and 8 particles per thread. No counterpart in the
+ * reference, which runs one domain per MPI job. */
+typedef struct pbpic_batch pbpic_batch;
+/* Creates the domains and loads them (cfgs[d], loaders[d]); each capacity is
+ * raised to the loader's particle count; cfgs[d].tile_rows 0 = default. */
+int pbpic_batch_create(const pbpic_config* cfgs, const pbpic_loader* loaders, int32_t ndomains,
+                       pbpic_batch** out);
+int pbpic_batch_destroy(pbpic_batch* b);
+int pbpic_batch_num_domains(const pbpic_batch* b, int32_t* n);
+/* The handle of domain d, owned by the batch: any read of the single-domain
+ * API works on it (store_particles_*, store_fields_f64, energies,
+ * energy_history, gauss_residual, ...). Do not destroy it or set its stream. */
+int pbpic_batch_domain(pbpic_batch* b, int32_t d, pbpic_handle** h);
+/* tile_rows: one per domain, 0 = default (NULL: all defaults), capped at 64
+ * and, with periodic y, at my - 2; groups: particles per thread / 4 (1 or 2). */
+int pbpic_batch_set_tiles(pbpic_batch* b, const int32_t* tile_rows, int32_t groups);
+int pbpic_batch_get_tiles(const pbpic_batch* b, int32_t* tile_rows, int32_t* groups);
+/* Enqueues nsteps steps of every domain on the batch's stream. */
+int pbpic_batch_step(pbpic_batch* b, int32_t nsteps);
+int pbpic_batch_synchronize(pbpic_batch* b);
+/* Times trial_steps steps (real steps of the run: every domain advances) for
+ * each candidate tiling (tile rows capped at 16, 32, 64; groups 1, 2), keeps
+ * the fastest and reports it. Either output may be NULL. The summation
+ * order of the FP32 current, and so its rounding, depends on the tiling. */
+int pbpic_batch_autotune(pbpic_batch* b, int32_t trial_steps, int32_t* tile_rows_out, int32_t* groups_out,
+                         double* best_ms_per_step);
+/* Energies (electron KE, ion KE, E, B) of every domain at its current step, ndomains x 4. */
+int pbpic_batch_energies(pbpic_batch* b, double* out);
+
 /* ------------------------------------------------------ differentiable form */
 /* Gradients of a time-integrated loss of the GEM Harris sheet with respect to
  * the perturbation amplitude psi0, the background density nb and T_i/T_e, by

@@ -107,6 +107,16 @@ SIGNATURES = {
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],
     "pbpic_kernel_launches": [_PI64],
     "pbpic_counting_sort_keys_static": [_P, _I64, _I32, _P, _P, _P],
+    "pbpic_batch_create": [ctypes.POINTER(Config), ctypes.POINTER(Loader), _I32, ctypes.POINTER(_P)],
+    "pbpic_batch_destroy": [_P],
+    "pbpic_batch_num_domains": [_P, _PI32],
+    "pbpic_batch_domain": [_P, _I32, ctypes.POINTER(_P)],
+    "pbpic_batch_set_tiles": [_P, _P, _I32],
+    "pbpic_batch_get_tiles": [_P, _P, _PI32],
+    "pbpic_batch_step": [_P, _I32],
+    "pbpic_batch_synchronize": [_P],
+    "pbpic_batch_autotune": [_P, _I32, _P, _PI32, _PD],
+    "pbpic_batch_energies": [_P, _P],
     "pbpic_diff_create": [ctypes.POINTER(DiffConfig), ctypes.POINTER(_P)],
     "pbpic_diff_destroy": [_P],
     "pbpic_diff_forward": [_P, ctypes.POINTER(DiffParams), _PD],

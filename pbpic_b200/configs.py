@@ -89,6 +89,60 @@ def harris_mid(seed=1):
     return harris(512, 256, 100, seed)
 
 
+ENSEMBLE_GRIDS = ((64, 64), (128, 64), (128, 128), (256, 128), (256, 256))
+
+
+def electron_scale(mx, my, ppc, mime=25.0, wpe_wce=2.0, dx_de=0.05, cfl=0.5):
+    """Periodic, unmagnetised electron-scale box: cells of dx_de electron
+    inertial lengths, the time step at Courant number cfl."""
+    cva = wpe_wce * math.sqrt(mime)
+    dx = dx_de / math.sqrt(mime)  # in d_i
+    return dict(mx=mx, my=my, dx=dx, dy=dx, dt=dt_for_cfl(cva, dx, dx, cfl), cva=cva, mime=mime,
+                in0=1.0 / ppc, ybc=L.BC_PERIODIC)
+
+
+def two_stream(mx, my, ppc, seed, vdrift=0.2, vthe=0.01):
+    """Electron two-stream: beams at +-vdrift c along x, electron thermal
+    speed vthe c, immobile neutralising ions."""
+    cfg = electron_scale(mx, my, ppc)
+    ld = dict(kind=L.LOAD_TWO_STREAM, ppc=ppc, vthe=vthe, vthi=0.0, vdrift_e=vdrift, immobile_ions=1, seed=seed)
+    return cfg, ld
+
+
+def weibel(mx, my, ppc, seed, anisotropy=8.0, vthe=0.1, mime=25.0):
+    """Weibel: electrons with T_perp / T_par = anisotropy (perpendicular
+    thermal speed vthe c), ions at the parallel electron temperature."""
+    cfg = electron_scale(mx, my, ppc, mime=mime)
+    vpar = vthe / math.sqrt(anisotropy)
+    ld = dict(kind=L.LOAD_WEIBEL, ppc=ppc, vthe=vthe, vthi=vpar / math.sqrt(mime), anisotropy=anisotropy,
+              seed=seed)
+    return cfg, ld
+
+
+def ensemble_c3(seed=2, n=64, grids=ENSEMBLE_GRIDS, ppc_range=(16, 128)):
+    """The batched ensemble: n instances, grids drawn from `grids`, 16 to 128
+    particles per cell per species; even instances two-stream (beams at
+    +-0.2 c, thermal 0.01 c), odd ones Weibel (T_perp/T_par = 8, thermal
+    0.1 c), drift and anisotropy jittered by +-20 % per instance."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        mx, my = grids[int(rng.integers(len(grids)))]
+        ppc = int(rng.integers(ppc_range[0], ppc_range[1] + 1))
+        jitter = 1.0 + 0.2 * float(rng.uniform(-1.0, 1.0))
+        inst_seed = 1000 * seed + i
+        if i % 2 == 0:
+            out.append(two_stream(mx, my, ppc, inst_seed, vdrift=0.2 * jitter))
+        else:
+            out.append(weibel(mx, my, ppc, inst_seed, anisotropy=8.0 * jitter))
+    return out
+
+
+def ensemble_particles(domains):
+    return sum(ld["ppc"] * c["mx"] * c["my"] * (1 if ld.get("immobile_ions") else 2) for c, ld in domains)
+
+
 WORKLOADS = {
     "uniform_128x128_ppc32": uniform_c1,
     "harris_1024x512_ppc100": harris_c2,

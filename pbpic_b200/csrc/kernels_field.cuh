@@ -28,6 +28,7 @@ struct FieldParams {
   double jscale[4];      // accumulator -> normalised current (in0, fixed-point scale)
   T* ng;                 // node grid (mx+1) x (my+1) x 8
   double* fe_part;       // per-block field energy partial sums [grid][2]
+  int nblk;              // batched launches: blocks that compute the partials
 };
 
 __device__ __forceinline__ int wrapx(int i, int mx) { return i < 0 ? i + mx : (i >= mx ? i - mx : i); }
@@ -54,7 +55,7 @@ __device__ __forceinline__ T node_row(const T* f, int i, int j, int my, int S, i
 
 // B half step, pic2d.f90:688-690 / 801-803, with the curl of E as in 790-793.
 template <class T>
-__global__ void k_bhalf(FieldParams<T> a) {
+__device__ __forceinline__ void bhalf_body(const FieldParams<T>& a) {
   const int rows = a.ybc == 0 ? a.my : a.my + 1;
   const long long n = (long long)a.mx * rows;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
@@ -82,6 +83,11 @@ __global__ void k_bhalf(FieldParams<T> a) {
   }
 }
 
+template <class T>
+__global__ void k_bhalf(FieldParams<T> a) {
+  bhalf_body(a);
+}
+
 template <class Acc>
 __device__ __forceinline__ double jval(const void* jacc, long long idx) {
   return (double)reinterpret_cast<const Acc*>(jacc)[idx];
@@ -89,7 +95,7 @@ __device__ __forceinline__ double jval(const void* jacc, long long idx) {
 
 // E full step, pic2d.f90:742-744 with the curl of B as in 733-739.
 template <class T, class Acc>
-__global__ void k_efull(FieldParams<T> a) {
+__device__ __forceinline__ void efull_body(const FieldParams<T>& a) {
   const int rows = a.ybc == 0 ? a.my : a.my + 1;
   const long long n = (long long)a.mx * rows;
   const long long plane = (long long)a.mx * a.S;
@@ -123,16 +129,21 @@ __global__ void k_efull(FieldParams<T> a) {
   }
 }
 
+template <class T, class Acc>
+__global__ void k_efull(FieldParams<T> a) {
+  efull_body<T, Acc>(a);
+}
+
 // Node averages (emfgrid, pic2d.f90:838-845) and the field energy sums
 // (pic2d.f90:659-670; with walls the two wall rows carry weight 1/2).
+// Block `bid` of `nblk` writes partial sums `bid` (the partition of the sums,
+// and so their rounding, depends only on nblk).
 template <class T>
-__global__ void k_nodes(FieldParams<T> a) {
-  __shared__ double red[32];
+__device__ __forceinline__ void nodes_body(const FieldParams<T>& a, double* red, int bid, int nblk) {
   const int NX = a.mx + 1, NY = a.my + 1;
   const long long n = (long long)NX * NY;
   double se = 0.0, sb = 0.0;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
+  for (long long k = bid * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)nblk * blockDim.x) {
     const int ia = (int)(k / NY), b = (int)(k - (long long)ia * NY);
     const int i = ia == a.mx ? 0 : ia;
     const int im = wrapx(i - 1, a.mx);
@@ -172,9 +183,39 @@ __global__ void k_nodes(FieldParams<T> a) {
   const double te = block_sum(se, red);
   const double tb = block_sum(sb, red);
   if (threadIdx.x == 0) {
-    a.fe_part[2 * blockIdx.x] = te;
-    a.fe_part[2 * blockIdx.x + 1] = tb;
+    a.fe_part[2 * bid] = te;
+    a.fe_part[2 * bid + 1] = tb;
   }
+}
+
+template <class T>
+__global__ void k_nodes(FieldParams<T> a) {
+  __shared__ double red[32];
+  nodes_body(a, red, blockIdx.x, gridDim.x);
+}
+
+// Batched domains: grid row blockIdx.y works on domain blockIdx.y.
+template <class T>
+__global__ void k_bhalf_batched(const FieldParams<T>* d) {
+  __shared__ FieldParams<T> a;
+  if (threadIdx.x == 0) a = d[blockIdx.y];
+  __syncthreads();
+  bhalf_body(a);
+}
+template <class T, class Acc>
+__global__ void k_efull_batched(const FieldParams<T>* d) {
+  __shared__ FieldParams<T> a;
+  if (threadIdx.x == 0) a = d[blockIdx.y];
+  __syncthreads();
+  efull_body<T, Acc>(a);
+}
+template <class T>
+__global__ void k_nodes_batched(const FieldParams<T>* d) {
+  __shared__ FieldParams<T> a;
+  __shared__ double red[32];
+  if (threadIdx.x == 0) a = d[blockIdx.y];
+  __syncthreads();
+  if ((int)blockIdx.x < a.nblk) nodes_body(a, red, blockIdx.x, a.nblk);
 }
 
 // Sum the per-tile kinetic and per-block field partials in a fixed order and
@@ -201,6 +242,36 @@ static __global__ void k_energy_row(const double* ke_part, int nke, const double
       if (c == 2 && fe_part) row[2] = t * fe_scale;
       if (c == 3 && fe_part) row[3] = t * fb_scale;
     }
+  }
+}
+
+// One energy row per domain (block blockIdx.x works on domain blockIdx.x),
+// written to row *step of the domain's rows (same sums as k_energy_row).
+struct EnergyRow {
+  const double* ke_part;
+  int nke;
+  const double* fe_part;
+  int nfe;
+  double fe_scale, fb_scale;
+  double* rows;
+};
+
+static __global__ void k_energy_rows_batched(const EnergyRow* d, const int* step) {
+  __shared__ double red[32];
+  const EnergyRow r = d[blockIdx.x];
+  double* row = r.rows + 4 * (long long)(*step);
+  double s[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < r.nke; i += blockDim.x) {
+    s[0] += r.ke_part[2 * i];
+    s[1] += r.ke_part[2 * i + 1];
+  }
+  for (int i = threadIdx.x; i < r.nfe; i += blockDim.x) {
+    s[2] += r.fe_part[2 * i];
+    s[3] += r.fe_part[2 * i + 1];
+  }
+  for (int c = 0; c < 4; ++c) {
+    const double t = block_sum(s[c], red);
+    if (threadIdx.x == 0) row[c] = c == 2 ? t * r.fe_scale : (c == 3 ? t * r.fb_scale : t);
   }
 }
 

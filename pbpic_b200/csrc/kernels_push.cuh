@@ -442,18 +442,17 @@ __device__ __forceinline__ void put4(V (&v)[4], int j, V x) {
   v[3] = j == 3 ? x : v[3];
 }
 
-// Dynamic shared memory: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
-template <class T, bool MIXED, bool HIST>
-__global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
+// Push of tile t of the domain `a`, by all threads of the block. G float4
+// groups of particles per thread per pass (8 particles for G = 2).
+// smem_raw: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
+template <class T, bool MIXED, bool HIST, int G>
+__device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T>& sm,
+                                          unsigned char* smem_raw) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
-  constexpr int G = PBPIC_PUSH_HALVES;  // float4 groups per thread per pass
-  constexpr int PT = 4 * G;             // particles per thread per pass
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ PushSmem<T> sm;
+  constexpr int PT = 4 * G;  // particles per thread per pass
   const int TY = a.tile_rows, WR = TY + 3, NB = 3 * (TY + 2);
   Acc* win = reinterpret_cast<Acc*>(smem_raw);
   int* hist = reinterpret_cast<int*>(win + 16 * WR);
-  const int t = blockIdx.x;
   const int ixt = t / a.tiles_per_col;
   const int y0 = (t - ixt * a.tiles_per_col) * TY;
   const int y1 = min(y0 + TY, a.my);
@@ -686,6 +685,36 @@ __global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_
   }
   status = __reduce_or_sync(FULL, status);
   if (lane == 0 && status) atomicOr(a.status, status);
+}
+
+// Single domain: one block per tile.
+template <class T, bool MIXED, bool HIST>
+__global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PushSmem<T> sm;
+  push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES>(a, blockIdx.x, sm, smem_raw);
+}
+
+// Batched domains: persistent blocks take (domain, tile) pairs from a global
+// counter (reset to 0 before each launch) in the order of `tiles`.
+template <class T, bool MIXED, bool HIST, int G>
+__global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
+    k_push_batched(const PushParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PushSmem<T> sm;
+  __shared__ PushParams<T> a;
+  __shared__ int next;
+  while (true) {
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = next;
+    if (t >= ntiles) break;
+    const int2 it = tiles[t];
+    if (threadIdx.x == 0) a = descs[it.x];
+    __syncthreads();
+    push_tile<T, MIXED, HIST, G>(a, it.y, sm, smem_raw);
+    __syncthreads();
+  }
 }
 
 }  // namespace pbd

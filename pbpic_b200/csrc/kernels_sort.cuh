@@ -273,7 +273,7 @@ struct FusedSortParams {
   int32_t* base;           // [ntiles][nb] first slot of each (tile, bin)
 };
 
-static __global__ void k_fused_counts(FusedSortParams a) {
+__device__ __forceinline__ void fused_counts_body(const FusedSortParams& a) {
   const int64_t ncells = (int64_t)a.mx * a.my;
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
     if (c == ncells) {
@@ -292,7 +292,9 @@ static __global__ void k_fused_counts(FusedSortParams a) {
   }
 }
 
-static __global__ void k_fused_base(FusedSortParams a) {
+static __global__ void k_fused_counts(FusedSortParams a) { fused_counts_body(a); }
+
+__device__ __forceinline__ void fused_base_body(const FusedSortParams& a) {
   const int64_t n = (int64_t)a.ntiles * a.nb;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int tt = (int)(e / a.nb), b = (int)(e - (int64_t)tt * a.nb);
@@ -318,6 +320,22 @@ static __global__ void k_fused_base(FusedSortParams a) {
   }
 }
 
+static __global__ void k_fused_base(FusedSortParams a) { fused_base_body(a); }
+
+static __global__ void k_fused_counts_batched(const FusedSortParams* d) {
+  __shared__ FusedSortParams a;
+  if (threadIdx.x == 0) a = d[blockIdx.y];
+  __syncthreads();
+  fused_counts_body(a);
+}
+
+static __global__ void k_fused_base_batched(const FusedSortParams* d) {
+  __shared__ FusedSortParams a;
+  if (threadIdx.x == 0) a = d[blockIdx.y];
+  __syncthreads();
+  fused_base_body(a);
+}
+
 template <class T>
 struct ScatterParams {
   int mx, my, ybc, ty, tpc, nb;
@@ -340,11 +358,16 @@ constexpr int SC_IPT = PBPIC_SCATTER_IPT, SC_CHUNK = 256 * SC_IPT, SC_MAXNB = 3 
 // [w*32*SC_IPT, (w+1)*32*SC_IPT), item k of lane l at k*32 + l, so
 // (warp, item, lane) order is array order. All loads of a chunk are issued
 // before the ranking so that they overlap.
+struct ScatterSmem {
+  int32_t cnt[8][SC_MAXNB];
+  int32_t run[SC_MAXNB], sbase[SC_MAXNB];
+};
+
 template <class T>
-__global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
-  __shared__ int32_t cnt[8][SC_MAXNB];
-  __shared__ int32_t run[SC_MAXNB], sbase[SC_MAXNB];
-  const int t = blockIdx.x;
+__device__ __forceinline__ void scatter_tile(const ScatterParams<T>& a, const int t, ScatterSmem& sm) {
+  int32_t(&cnt)[8][SC_MAXNB] = sm.cnt;
+  int32_t* run = sm.run;
+  int32_t* sbase = sm.sbase;
   const int ixt = t / a.tpc, y0 = (t - ixt * a.tpc) * a.ty, y1 = min(y0 + a.ty, a.my);
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
   const int w = threadIdx.x >> 5;
@@ -415,6 +438,56 @@ __global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
       }
     }
     __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
+  __shared__ ScatterSmem sm;
+  scatter_tile(a, blockIdx.x, sm);
+}
+
+// Batched domains: persistent blocks take (domain, tile) pairs from a counter.
+template <class T>
+__global__ void __launch_bounds__(256)
+    k_fused_scatter_batched(const ScatterParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
+  __shared__ ScatterSmem sm;
+  __shared__ ScatterParams<T> a;
+  __shared__ int next;
+  while (true) {
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = next;
+    if (t >= ntiles) break;
+    const int2 it = tiles[t];
+    if (threadIdx.x == 0) a = descs[it.x];
+    __syncthreads();
+    scatter_tile(a, it.y, sm);
+    __syncthreads();
+  }
+}
+
+}  // namespace pbd
+
+namespace pbd {
+
+// Tile ranges of batched domains (grid row blockIdx.y = domain).
+struct TileOffDesc {
+  const int32_t* off;  // the domain's cell offsets (global positions)
+  int ntiles, tpc, ty, my;
+  int32_t end;         // global position after the domain's last particle
+  int32_t* tile_off;
+};
+
+static __global__ void k_tile_off_batched(const TileOffDesc* d) {
+  const TileOffDesc a = d[blockIdx.y];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= a.ntiles; t += gridDim.x * blockDim.x) {
+    if (t == a.ntiles) {
+      a.tile_off[t] = a.end;
+    } else {
+      const int ix = t / a.tpc;
+      a.tile_off[t] = a.off[(int64_t)ix * a.my + (int64_t)(t - ix * a.tpc) * a.ty];
+    }
   }
 }
 

@@ -14,6 +14,7 @@
 #include "../../include/pbpic.h"
 #include "api_internal.h"
 #include "device_common.cuh"
+#include "kernels_batch.cuh"
 #include "kernels_field.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_push.cuh"
@@ -157,6 +158,8 @@ struct pbpic_handle {
   bool fused_ok = false;    // grid admits the fused counting sort (distinct window cells)
   bool hist_valid = false;  // the last push counted new cells per tile on a sorted array
   int nb = 0;               // window bins per tile, 3*(TY+2)
+  int tile_cap = 0;         // tiles the per-tile arrays hold
+  int64_t bin_cap = 0;      // (tile, bin) entries tilecnt and tbase hold
   int32_t* tilecnt = nullptr;
   int32_t* tbase = nullptr;
   void* staging = nullptr;
@@ -769,6 +772,8 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
   A(&h->tilecnt, (size_t)h->ntiles * h->nb * 4);
   A(&h->tbase, (size_t)h->ntiles * h->nb * 4);
   A(&h->ke_part, (size_t)std::max(h->ntiles, 148 * 16) * 2 * 8);
+  h->tile_cap = h->ntiles;
+  h->bin_cap = (int64_t)h->ntiles * h->nb;
   h->nke = 148 * 8;
   h->nfe = grid_for((int64_t)(c.mx + 1) * (c.my + 1), 256, 148 * 8);
   A(&h->fe_part, (size_t)h->nfe * 2 * 8);
@@ -1155,3 +1160,554 @@ extern "C" int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t 
   if (st & 8) return fail(PBPIC_EINVAL, "key outside [0, ncells)");
   return PBPIC_OK;
 }
+
+// ============================================================== batched form
+// Many independent FP32 domains advanced together. Every domain is an
+// ordinary handle (its own particles, fields and tables); a batched step runs
+// each phase once for all domains:
+//   k_batch_begin          zero the current accumulators, reset counters
+//   k_push_batched         persistent blocks over the (domain, tile) table
+//   k_fused_counts_batched, k_scan_batched, k_fused_base_batched,
+//   k_fused_scatter_batched (persistent), k_tile_off_batched
+//                          the fused counting sort of every domain
+//   k_bhalf/k_efull/k_bhalf/k_nodes_batched, k_energy_rows_batched
+// Two consecutive steps (the particle buffers swap each step) are captured
+// once in a CUDA graph and replayed. A domain stepped here goes through the
+// same arithmetic as pbpic_step(h, n, 1) with the same tile rows and
+// particles per thread, so its state is bit-identical to that run.
+struct pbpic_batch {
+  std::vector<pbpic_handle*> dom;
+  cudaStream_t stream = nullptr;
+  int groups = PBPIC_PUSH_HALVES;  // particles per thread / 4 in the push
+  int64_t launches_per_pair = 0;
+  cudaGraphExec_t graph = nullptr;
+  // descriptor tables: host copies (kept alive for the asynchronous uploads) and device arrays
+  std::vector<PushParams<float>> h_push;       // [2][D]: [0] the domains' current buffers, [1] swapped
+  std::vector<ScatterParams<float>> h_scat;    // [2][D]
+  std::vector<FusedSortParams> h_fsort;
+  std::vector<FieldParams<float>> h_field;
+  std::vector<TileOffDesc> h_toff;
+  std::vector<BatchDomain> h_dom;
+  std::vector<EnergyRow> h_erow;
+  std::vector<int2> h_tiles;
+  PushParams<float>* d_push = nullptr;
+  ScatterParams<float>* d_scat = nullptr;
+  FusedSortParams* d_fsort = nullptr;
+  FieldParams<float>* d_field = nullptr;
+  TileOffDesc* d_toff = nullptr;
+  BatchDomain* d_dom = nullptr;
+  EnergyRow* d_erow = nullptr;
+  int2* d_tiles = nullptr;
+  int* d_counters = nullptr;  // [0] push, [1] scatter, [2] step index
+  int ntiles = 0, push_blocks = 0, scatter_blocks = 0;
+  size_t push_smem = 0;
+  int gx_zero = 1, gx_cells = 1, gx_bins = 1, gx_tiles = 1, gx_field = 1, gx_nodes = 1;
+};
+
+namespace {
+
+void dfree(pbpic_handle* h, void* p) {
+  if (!p) return;
+  cudaFree(p);
+  auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+  if (it != h->allocs.end()) h->allocs.erase(it);
+}
+
+// Tile rows of a domain: ty, or the default for ty <= 0, capped so that the
+// fused counting sort applies (with periodic y a tile's window must hold
+// distinct rows).
+int batch_tile_rows(const pbpic_handle* h, int ty) {
+  const pbpic_config& c = h->cfg;
+  const int cap = c.ybc == PBPIC_BC_PERIODIC ? std::max(1, std::min(64, c.my - 2)) : std::min(64, c.my);
+  return ty > 0 ? std::min(ty, cap) : cap;
+}
+
+// Change a handle's tile rows, growing its per-tile arrays if needed, and
+// recompute its tile ranges (from the cell offsets when sorted).
+int retile(pbpic_handle* h, int ty) {
+  if (ty == h->TY) return PBPIC_OK;
+  const pbpic_config& c = h->cfg;
+  const int tpc = (c.my + ty - 1) / ty;
+  const int ntiles = c.mx * tpc;
+  const int nb = 3 * (ty + 2);
+  CK(cudaStreamSynchronize(h->stream));
+  if (ntiles > h->tile_cap) {
+    dfree(h, h->tile_off);
+    dfree(h, h->ke_part);
+    h->tile_off = nullptr;
+    h->ke_part = nullptr;
+    TRY(dalloc(h, &h->tile_off, (size_t)(ntiles + 1) * 4));
+    TRY(dalloc(h, &h->ke_part, (size_t)std::max(ntiles, 148 * 16) * 2 * 8));
+    h->tile_cap = ntiles;
+  }
+  if ((int64_t)ntiles * nb > h->bin_cap) {
+    dfree(h, h->tilecnt);
+    dfree(h, h->tbase);
+    h->tilecnt = nullptr;
+    h->tbase = nullptr;
+    TRY(dalloc(h, &h->tilecnt, (size_t)ntiles * nb * 4));
+    TRY(dalloc(h, &h->tbase, (size_t)ntiles * nb * 4));
+    h->bin_cap = (int64_t)ntiles * nb;
+  }
+  h->TY = ty;
+  h->tpc = tpc;
+  h->ntiles = ntiles;
+  h->nb = nb;
+  h->fused_ok = c.mx >= 3 && (c.ybc == PBPIC_BC_CONDUCTING || c.my >= ty + 2);
+  h->hist_valid = false;
+  if (h->sorted) {
+    k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, h->stream>>>(h->off, h->ntiles, h->tpc, h->TY,
+                                                                            c.my, (int32_t)h->n, h->tile_off);
+    CKLAUNCH("k_tile_off");
+  } else {
+    TRY(set_unsorted_tiles(h));
+  }
+  return PBPIC_OK;
+}
+
+void drop_graph(pbpic_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+template <class X>
+int upload(pbpic_batch* b, X* dst, const std::vector<X>& src) {
+  if (src.empty()) return PBPIC_OK;
+  CK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(X), cudaMemcpyHostToDevice, b->stream));
+  return PBPIC_OK;
+}
+
+// Build the (domain, tile) table, largest expected tiles first (rows x mean
+// particles per cell), and the launch shapes. Called when tile rows change.
+int batch_layout(pbpic_batch* b) {
+  const int D = (int)b->dom.size();
+  struct Item {
+    double cost;
+    int d, t;
+  };
+  std::vector<Item> items;
+  size_t smem = 0;
+  int64_t maxcells = 1, maxbins = 1, maxtiles = 1, maxfield = 1, maxacc = 1;
+  int maxnfe = 1;
+  for (int d = 0; d < D; ++d) {
+    const pbpic_handle* h = b->dom[d];
+    const double ppc = (double)h->n / (double)h->ncells;
+    for (int t = 0; t < h->ntiles; ++t) {
+      const int y0 = (t % h->tpc) * h->TY;
+      const int rows = std::min(h->TY, h->cfg.my - y0);
+      items.push_back({rows * ppc, d, t});
+    }
+    smem = std::max(smem, (size_t)16 * (h->TY + 3) * 8 + (size_t)h->nb * 4);
+    maxcells = std::max<int64_t>(maxcells, (int64_t)h->ncells + 1);
+    maxbins = std::max<int64_t>(maxbins, (int64_t)h->ntiles * h->nb);
+    maxtiles = std::max<int64_t>(maxtiles, (int64_t)h->ntiles + 1);
+    const int rows = h->cfg.ybc == 0 ? h->cfg.my : h->cfg.my + 1;
+    maxfield = std::max<int64_t>(maxfield, (int64_t)h->cfg.mx * rows);
+    maxacc = std::max<int64_t>(maxacc, 2 * plane_elems(h));  // 16-byte stores of 4 planes
+    maxnfe = std::max(maxnfe, h->nfe);
+  }
+  std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+  if (items.size() > (size_t)0x7fffffff) return fail(PBPIC_EINVAL, "too many tiles in the batch");
+  b->h_tiles.resize(items.size());
+  for (size_t k = 0; k < items.size(); ++k) b->h_tiles[k] = make_int2(items[k].d, items[k].t);
+  b->ntiles = (int)items.size();
+  b->push_smem = smem;
+  if (b->d_tiles) cudaFree(b->d_tiles);
+  b->d_tiles = nullptr;
+  CK(cudaMalloc(&b->d_tiles, std::max<size_t>(1, items.size()) * sizeof(int2)));
+  TRY(upload(b, b->d_tiles, b->h_tiles));
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int per_sm = 1;
+  if (b->groups == 1) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 1>, NTHREADS, smem));
+  } else {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 2>, NTHREADS, smem));
+  }
+  b->push_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_scatter_batched<float>, 256, 0));
+  b->scatter_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
+  b->gx_zero = grid_for(maxacc, 256, 1024);
+  b->gx_cells = grid_for(maxcells, 256);
+  b->gx_bins = grid_for(maxbins, 256);
+  b->gx_tiles = grid_for(maxtiles, 256, 1 << 16);
+  b->gx_field = grid_for(maxfield, 256);
+  b->gx_nodes = maxnfe;
+  (void)D;
+  return PBPIC_OK;
+}
+
+// Descriptor tables from the domains' current state (buffers, histories).
+int batch_descriptors(pbpic_batch* b) {
+  const int D = (int)b->dom.size();
+  b->h_push.resize(2 * D);
+  b->h_scat.resize(2 * D);
+  b->h_fsort.resize(D);
+  b->h_field.resize(D);
+  b->h_toff.resize(D);
+  b->h_dom.resize(D);
+  b->h_erow.resize(D);
+  for (int d = 0; d < D; ++d) {
+    pbpic_handle* h = b->dom[d];
+    const int cur0 = h->cur;
+    for (int par = 0; par < 2; ++par) {
+      h->cur = par == 0 ? cur0 : 1 - cur0;
+      b->h_push[par * D + d] = push_params<float, true>(h);
+      const int i = h->cur, o = 1 - i;
+      ScatterParams<float>& sp = b->h_scat[par * D + d];
+      sp.mx = h->cfg.mx;
+      sp.my = h->cfg.my;
+      sp.ybc = h->cfg.ybc;
+      sp.ty = h->TY;
+      sp.tpc = h->tpc;
+      sp.nb = h->nb;
+      sp.tile_off = h->tile_off;
+      sp.base = h->tbase;
+      sp.ci = h->cell[i];
+      sp.dxi = P<float>(h, i, 0);
+      sp.dyi = P<float>(h, i, 1);
+      sp.uxi = P<float>(h, i, 2);
+      sp.uyi = P<float>(h, i, 3);
+      sp.uzi = P<float>(h, i, 4);
+      sp.pidi = h->pid[i];
+      sp.co = h->cell[o];
+      sp.dxo = P<float>(h, o, 0);
+      sp.dyo = P<float>(h, o, 1);
+      sp.uxo = P<float>(h, o, 2);
+      sp.uyo = P<float>(h, o, 3);
+      sp.uzo = P<float>(h, o, 4);
+      sp.pido = h->pid[o];
+    }
+    h->cur = cur0;
+    FusedSortParams& f = b->h_fsort[d];
+    f.mx = h->cfg.mx;
+    f.my = h->cfg.my;
+    f.ybc = h->cfg.ybc;
+    f.ty = h->TY;
+    f.tpc = h->tpc;
+    f.ntiles = h->ntiles;
+    f.nb = h->nb;
+    f.tilecnt = h->tilecnt;
+    f.counts = h->counts;
+    f.off = h->off;
+    f.base = h->tbase;
+    b->h_field[d] = field_params<float, true>(h);
+    b->h_field[d].nblk = h->nfe;
+    TileOffDesc& t = b->h_toff[d];
+    t.off = h->off;
+    t.ntiles = h->ntiles;
+    t.tpc = h->tpc;
+    t.ty = h->TY;
+    t.my = h->cfg.my;
+    t.end = (int32_t)h->n;
+    t.tile_off = h->tile_off;
+    BatchDomain& bd = b->h_dom[d];
+    bd.jacc = (long long*)h->jacc;
+    bd.nacc = 4 * plane_elems(h);
+    bd.counts = h->counts;
+    bd.off = h->off;
+    bd.ncounts = h->ncells + 1;
+    EnergyRow& e = b->h_erow[d];
+    e.ke_part = h->ke_part;
+    e.nke = h->ntiles;
+    e.fe_part = h->fe_part;
+    e.nfe = h->nfe;
+    e.fe_scale = fe_scale(h->cfg);
+    e.fb_scale = fb_scale(h->cfg);
+    e.rows = h->hist + (size_t)(h->itime + 1) * 4;
+  }
+  TRY(upload(b, b->d_push, b->h_push));
+  TRY(upload(b, b->d_scat, b->h_scat));
+  TRY(upload(b, b->d_fsort, b->h_fsort));
+  TRY(upload(b, b->d_field, b->h_field));
+  TRY(upload(b, b->d_toff, b->h_toff));
+  TRY(upload(b, b->d_dom, b->h_dom));
+  TRY(upload(b, b->d_erow, b->h_erow));
+  return PBPIC_OK;
+}
+
+// One batched step on descriptor set `par` (0: buffers as uploaded, 1: swapped).
+int batch_enqueue_step(pbpic_batch* b, int par) {
+  const int D = (int)b->dom.size();
+  cudaStream_t s = b->stream;
+  int* ctr = b->d_counters;
+  k_batch_begin<<<dim3(b->gx_zero, D), 256, 0, s>>>(b->d_dom, ctr, ctr + 2);
+  CKLAUNCH("k_batch_begin");
+  const PushParams<float>* pp = b->d_push + (size_t)par * D;
+  if (b->groups == 1)
+    k_push_batched<float, true, true, 1><<<b->push_blocks, NTHREADS, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+  else
+    k_push_batched<float, true, true, 2><<<b->push_blocks, NTHREADS, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+  CKLAUNCH("k_push_batched");
+  k_fused_counts_batched<<<dim3(b->gx_cells, D), 256, 0, s>>>(b->d_fsort);
+  CKLAUNCH("k_fused_counts_batched");
+  k_scan_batched<<<D, SCB, 0, s>>>(b->d_dom);
+  CKLAUNCH("k_scan_batched");
+  k_fused_base_batched<<<dim3(b->gx_bins, D), 256, 0, s>>>(b->d_fsort);
+  CKLAUNCH("k_fused_base_batched");
+  k_fused_scatter_batched<float><<<b->scatter_blocks, 256, 0, s>>>(b->d_scat + (size_t)par * D, b->d_tiles,
+                                                                   b->ntiles, ctr + 1);
+  CKLAUNCH("k_fused_scatter_batched");
+  k_tile_off_batched<<<dim3(b->gx_tiles, D), 256, 0, s>>>(b->d_toff);
+  CKLAUNCH("k_tile_off_batched");
+  k_bhalf_batched<float><<<dim3(b->gx_field, D), 256, 0, s>>>(b->d_field);
+  CKLAUNCH("k_bhalf_batched");
+  k_efull_batched<float, long long><<<dim3(b->gx_field, D), 256, 0, s>>>(b->d_field);
+  CKLAUNCH("k_efull_batched");
+  k_bhalf_batched<float><<<dim3(b->gx_field, D), 256, 0, s>>>(b->d_field);
+  CKLAUNCH("k_bhalf_batched");
+  k_nodes_batched<float><<<dim3(b->gx_nodes, D), 256, 0, s>>>(b->d_field);
+  CKLAUNCH("k_nodes_batched");
+  k_energy_rows_batched<<<D, 256, 0, s>>>(b->d_erow, ctr + 2);
+  CKLAUNCH("k_energy_rows_batched");
+  return PBPIC_OK;
+}
+
+// Capture two consecutive steps (set 0 then set 1) into a graph.
+int batch_capture(pbpic_batch* b) {
+  drop_graph(b);
+  const long long before = g_launches.load();
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int r = batch_enqueue_step(b, 0);
+  if (r == PBPIC_OK) r = batch_enqueue_step(b, 1);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  const long long captured = g_launches.load() - before;
+  g_launches.fetch_sub(captured);  // counted again at each replay
+  if (r != PBPIC_OK) {
+    if (g) cudaGraphDestroy(g);
+    return r;
+  }
+  if (e != cudaSuccess) return fail(PBPIC_ECUDA, std::string("stream capture of the batched step: ") + cudaGetErrorString(e));
+  const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    b->graph = nullptr;
+    return fail(PBPIC_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+  }
+  b->launches_per_pair = captured;
+  return PBPIC_OK;
+}
+
+int batch_set_tiles(pbpic_batch* b, const int32_t* tile_rows, int groups) {
+  if (groups != 1 && groups != 2) return fail(PBPIC_EINVAL, "groups (particles per thread / 4) must be 1 or 2");
+  for (size_t d = 0; d < b->dom.size(); ++d) {
+    pbpic_handle* h = b->dom[d];
+    TRY(retile(h, batch_tile_rows(h, tile_rows ? tile_rows[d] : 0)));
+  }
+  b->groups = groups;
+  drop_graph(b);
+  return batch_layout(b);
+}
+
+int batch_step(pbpic_batch* b, int nsteps) {
+  if (nsteps <= 0) return PBPIC_OK;
+  for (pbpic_handle* h : b->dom) {
+    if (!h->sorted) TRY(do_sort<float, true>(h));
+    TRY(ensure_hist(h, h->itime + nsteps + 2));
+  }
+  TRY(batch_descriptors(b));
+  CK(cudaMemsetAsync(b->d_counters + 2, 0xff, sizeof(int), b->stream));  // step index -1
+  if (nsteps >= 2 && !b->graph) TRY(batch_capture(b));
+  for (int k = 0; k + 1 < nsteps; k += 2) {
+    CK(cudaGraphLaunch(b->graph, b->stream));
+    g_launches.fetch_add(b->launches_per_pair);
+  }
+  if (nsteps & 1) TRY(batch_enqueue_step(b, 0));
+  for (pbpic_handle* h : b->dom) {
+    if (nsteps & 1) h->cur = 1 - h->cur;
+    h->itime += nsteps;
+    h->sorted = true;
+    h->hist_valid = false;
+  }
+  return PBPIC_OK;
+}
+
+int check_batch(const pbpic_batch* b) {
+  if (!b) return fail(PBPIC_EINVAL, "null batch");
+  return PBPIC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbpic_batch_destroy(pbpic_batch* b) {
+  if (!b) return PBPIC_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graph(b);
+  for (pbpic_handle* h : b->dom) {
+    h->stream = 0;
+    pbpic_destroy(h);
+  }
+  void* arrays[] = {b->d_push, b->d_scat, b->d_fsort, b->d_field, b->d_toff, b->d_dom, b->d_erow, b->d_tiles,
+                    b->d_counters};
+  for (void* p : arrays)
+    if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return PBPIC_OK;
+}
+
+int pbpic_batch_create(const pbpic_config* cfgs, const pbpic_loader* loaders, int32_t ndomains, pbpic_batch** out) {
+  if (!cfgs || !loaders || !out) return fail(PBPIC_EINVAL, "null argument");
+  *out = nullptr;
+  if (ndomains < 1 || ndomains > 65535) return fail(PBPIC_EINVAL, "ndomains must be in [1, 65535]");
+  for (int d = 0; d < ndomains; ++d) {
+    const pbpic_config& c = cfgs[d];
+    if (c.precision != PBPIC_FP32_MIXED) return fail(PBPIC_EINVAL, "the batched form runs FP32 mixed domains only");
+    if (c.mx < 3 || (c.ybc == PBPIC_BC_PERIODIC && c.my < 3))
+      return fail(PBPIC_EINVAL, "batched domains need mx >= 3, and my >= 3 with periodic y");
+  }
+  pbpic_batch* b = new pbpic_batch();
+  auto bail = [&](int r) {
+    pbpic_batch_destroy(b);
+    return r;
+  };
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    b->stream = nullptr;
+    return bail(fail(PBPIC_ECUDA, "cudaStreamCreateWithFlags failed"));
+  }
+  for (int d = 0; d < ndomains; ++d) {
+    pbpic_config c = cfgs[d];
+    const int64_t pairs = (int64_t)loaders[d].ppc * c.mx * c.my;
+    const int64_t need = loaders[d].immobile_ions ? pairs : 2 * pairs;
+    c.capacity = std::max<int64_t>(c.capacity, need);
+    c.tile_rows = 0;
+    pbpic_handle* h = nullptr;
+    int r = pbpic_create(&c, &h);
+    if (r != PBPIC_OK) return bail(r);
+    h->cfg.tile_rows = cfgs[d].tile_rows;
+    h->stream = b->stream;
+    b->dom.push_back(h);
+    r = do_init_plasma<float, true>(h, &loaders[d]);
+    if (r != PBPIC_OK) {
+      g_err = "domain " + std::to_string(d) + ": " + g_err;
+      return bail(r);
+    }
+  }
+  const size_t D = (size_t)ndomains;
+  int r = PBPIC_OK;
+  auto M = [&](auto** p, size_t bytes) {
+    if (r == PBPIC_OK && cudaMalloc((void**)p, bytes) != cudaSuccess) {
+      *p = nullptr;
+      r = fail(PBPIC_ENOMEM, "cudaMalloc of the batch tables failed");
+    }
+  };
+  M(&b->d_push, 2 * D * sizeof(PushParams<float>));
+  M(&b->d_scat, 2 * D * sizeof(ScatterParams<float>));
+  M(&b->d_fsort, D * sizeof(FusedSortParams));
+  M(&b->d_field, D * sizeof(FieldParams<float>));
+  M(&b->d_toff, D * sizeof(TileOffDesc));
+  M(&b->d_dom, D * sizeof(BatchDomain));
+  M(&b->d_erow, D * sizeof(EnergyRow));
+  M(&b->d_counters, 4 * sizeof(int));
+  if (r != PBPIC_OK) return bail(r);
+  std::vector<int32_t> ty(D);
+  for (size_t d = 0; d < D; ++d) ty[d] = cfgs[d].tile_rows;
+  r = batch_set_tiles(b, ty.data(), PBPIC_PUSH_HALVES);
+  if (r != PBPIC_OK) return bail(r);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(fail(PBPIC_ECUDA, "batch initialisation failed"));
+  *out = b;
+  return PBPIC_OK;
+}
+
+int pbpic_batch_num_domains(const pbpic_batch* b, int32_t* n) {
+  TRY(check_batch(b));
+  if (!n) return fail(PBPIC_EINVAL, "null argument");
+  *n = (int32_t)b->dom.size();
+  return PBPIC_OK;
+}
+
+int pbpic_batch_domain(pbpic_batch* b, int32_t d, pbpic_handle** h) {
+  TRY(check_batch(b));
+  if (!h) return fail(PBPIC_EINVAL, "null argument");
+  if (d < 0 || d >= (int32_t)b->dom.size()) return fail(PBPIC_EINVAL, "domain index out of range");
+  *h = b->dom[d];
+  return PBPIC_OK;
+}
+
+int pbpic_batch_set_tiles(pbpic_batch* b, const int32_t* tile_rows, int32_t groups) {
+  TRY(check_batch(b));
+  return batch_set_tiles(b, tile_rows, groups);
+}
+
+int pbpic_batch_get_tiles(const pbpic_batch* b, int32_t* tile_rows, int32_t* groups) {
+  TRY(check_batch(b));
+  if (tile_rows)
+    for (size_t d = 0; d < b->dom.size(); ++d) tile_rows[d] = b->dom[d]->TY;
+  if (groups) *groups = b->groups;
+  return PBPIC_OK;
+}
+
+int pbpic_batch_step(pbpic_batch* b, int32_t nsteps) {
+  TRY(check_batch(b));
+  if (nsteps < 0) return fail(PBPIC_EINVAL, "nsteps must be >= 0");
+  return batch_step(b, nsteps);
+}
+
+int pbpic_batch_synchronize(pbpic_batch* b) {
+  TRY(check_batch(b));
+  CK(cudaStreamSynchronize(b->stream));
+  return PBPIC_OK;
+}
+
+int pbpic_batch_autotune(pbpic_batch* b, int32_t trial_steps, int32_t* tile_rows_out, int32_t* groups_out,
+                         double* best_ms_per_step) {
+  TRY(check_batch(b));
+  if (trial_steps < 2) return fail(PBPIC_EINVAL, "trial_steps must be >= 2");
+  const int pairs = trial_steps / 2;
+  const int caps[] = {16, 32, 64};
+  const int D = (int)b->dom.size();
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e300;
+  int best_cap = 64, best_g = PBPIC_PUSH_HALVES;
+  std::vector<int32_t> ty(D);
+  int r = PBPIC_OK;
+  for (int g = 1; g <= 2 && r == PBPIC_OK; ++g)
+    for (int cap : caps) {
+      for (int d = 0; d < D; ++d) ty[d] = cap;
+      r = batch_set_tiles(b, ty.data(), g);
+      if (r == PBPIC_OK) r = batch_step(b, 2);  // capture and warm up
+      if (r == PBPIC_OK && cudaEventRecord(e0, b->stream) != cudaSuccess) r = fail(PBPIC_ECUDA, "cudaEventRecord");
+      if (r == PBPIC_OK) r = batch_step(b, 2 * pairs);
+      if (r == PBPIC_OK && cudaEventRecord(e1, b->stream) != cudaSuccess) r = fail(PBPIC_ECUDA, "cudaEventRecord");
+      float ms = 0;
+      if (r == PBPIC_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        r = fail(PBPIC_ECUDA, "timing the autotuner trial failed");
+      if (r != PBPIC_OK) break;
+      const double per = ms / (2.0 * pairs);
+      if (per < best) {
+        best = per;
+        best_cap = cap;
+        best_g = g;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  TRY(r);
+  for (int d = 0; d < D; ++d) ty[d] = best_cap;
+  TRY(batch_set_tiles(b, ty.data(), best_g));
+  if (tile_rows_out)
+    for (int d = 0; d < D; ++d) tile_rows_out[d] = b->dom[d]->TY;
+  if (groups_out) *groups_out = best_g;
+  if (best_ms_per_step) *best_ms_per_step = best;
+  return PBPIC_OK;
+}
+
+int pbpic_batch_energies(pbpic_batch* b, double* out) {
+  TRY(check_batch(b));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  for (size_t d = 0; d < b->dom.size(); ++d) {
+    const pbpic_handle* h = b->dom[d];
+    CK(cudaMemcpyAsync(out + 4 * d, h->hist + (size_t)h->itime * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                       b->stream));
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  return PBPIC_OK;
+}
+
+}  // extern "C"

@@ -26,6 +26,20 @@ class Simulation:
         L.check(self._lib.pbpic_create(ctypes.byref(self.cfg), ctypes.byref(self._h)))
 
     @classmethod
+    def _borrow(cls, handle):
+        """A view of a handle owned elsewhere (a domain of a Batch); closing
+        the view leaves the handle alive."""
+        self = cls.__new__(cls)
+        self._lib = L.lib()
+        self._h = ctypes.c_void_p(handle)
+        self._owned = False
+        self.cfg = L.Config()
+        L.check(self._lib.pbpic_get_config(self._h, ctypes.byref(self.cfg)))
+        self.mx, self.my = self.cfg.mx, self.cfg.my
+        self.precision = "fp32" if self.cfg.precision == L.FP32_MIXED else "fp64"
+        return self
+
+    @classmethod
     def from_config(cls, cfg, **kw):
         args = dict(cfg)
         args.update(kw)
@@ -33,9 +47,9 @@ class Simulation:
 
     # --------------------------------------------------------------- lifecycle
     def close(self):
-        if self._h:
+        if self._h and getattr(self, "_owned", True):
             self._lib.pbpic_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __enter__(self):
         return self

@@ -67,3 +67,24 @@ def test_create_reports_errors_without_crashing():
     with pytest.raises(pbpic_b200.PbpicError) as e:
         pbpic_b200.Simulation(**dict(cfg, dt=cfg["dt"] * 4))
     assert "CFL" in str(e.value)
+
+
+def test_batch_create_rejects_bad_domains_before_device_work():
+    """The batched form takes FP32 mixed domains with mx >= 3 (and my >= 3 with periodic y)."""
+    import pbpic_b200
+    from pbpic_b200 import _lib, configs
+    from pbpic_b200.batch import Batch
+    cfg, ld = configs.two_stream(8, 8, 4, seed=1)
+    with pytest.raises(pbpic_b200.PbpicError) as e:
+        Batch([(cfg, ld), (dict(cfg, mx=2), ld)])
+    assert "mx >= 3" in str(e.value)
+    lib = _lib.lib()
+    cfgs = (_lib.Config * 1)()
+    for k, v in cfg.items():
+        setattr(cfgs[0], k, v)
+    cfgs[0].precision = _lib.FP64_PLAIN
+    loaders = (_lib.Loader * 1)()
+    out = ctypes.c_void_p()
+    assert lib.pbpic_batch_create(cfgs, loaders, 1, ctypes.byref(out)) == -1
+    assert b"FP32" in lib.pbpic_last_error()
+    assert lib.pbpic_batch_create(cfgs, loaders, 0, ctypes.byref(out)) == -1
