@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--sort-every", type=int, default=1)
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=20)
     return ap.parse_args()
 
 
@@ -185,7 +187,13 @@ def run_gpu(args, rank, world, dist):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, cfg, ld, stream, barrier, max_over_ranks)
-    return cfg, results, clocks, e2e
+    ens = None
+    if not args.no_ensemble and world == 1:
+        try:
+            ens = run_ensemble(args)
+        except Exception as exc:  # reported in the line; the headline stands on its own
+            ens = dict(error=f"{type(exc).__name__}: {exc}")
+    return cfg, results, clocks, e2e, ens
 
 
 def run_e2e(args, cfg, ld, stream, barrier, max_over_ranks):
@@ -221,6 +229,51 @@ def run_e2e(args, cfg, ld, stream, barrier, max_over_ranks):
         dt = time.perf_counter() - t0
     dt = max_over_ranks(dt)
     return dict(seconds=dt, n=n, K=K, h2d=n * 32 / K, d2h=32 + n * 32 / K)
+
+
+def run_ensemble(args):
+    """The batched ensemble: 64 two-stream / Weibel instances of uneven size
+    (194M particles in all), FP32. Tiles autotuned (its trial steps are steps
+    of the run), then K batched steps timed with CUDA events on the batch's
+    stream, against K steps of the same domains launched one instance at a
+    time (pbpic_step per domain, the same tiles)."""
+    import torch
+
+    from pbpic_b200 import configs
+    from pbpic_b200.batch import Batch
+    from pbpic_b200.sim import kernel_launches
+    doms = configs.ensemble_c3()
+    n = configs.ensemble_particles(doms)
+    K = args.ensemble_steps
+    with Batch(doms) as b:
+        st = torch.cuda.ExternalStream(b.stream)
+        tiles, groups, tune_ms = b.autotune(8)
+        b.step(max(2, args.warmup))
+        b.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        l0 = kernel_launches()
+        ev[0].record(st)
+        b.step(K)
+        ev[1].record(st)
+        b.synchronize()
+        l1 = kernel_launches()
+        sims = [b.domain(d) for d in range(len(doms))]
+        ev[2].record(st)
+        for _ in range(K):
+            for s in sims:
+                s.step(1, sort_every=1)
+        ev[3].record(st)
+        b.synchronize()
+        l2 = kernel_launches()
+        t_batch = ev[0].elapsed_time(ev[1])
+        t_single = ev[2].elapsed_time(ev[3])
+        gauss = max(s.gauss_residual() for s in sims[1::2])  # Weibel: mobile ions, residual starts at 0
+        status = 0
+        for s in sims:
+            status |= s.status()
+        return dict(n=n, K=K, t_batch=t_batch, t_single=t_single, tiles=sorted(set(int(t) for t in tiles)),
+                    groups=groups, tune_ms=tune_ms, launches_batch=l1 - l0, launches_single=l2 - l1,
+                    gauss=gauss, status=status)
 
 
 # ---------------------------------------------------------------------- CPU
@@ -286,7 +339,7 @@ def main():
         import torch.distributed as tdist
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
-    cfg, res, clocks, e2e = run_gpu(args, rank, world, dist)
+    cfg, res, clocks, e2e, ens = run_gpu(args, rank, world, dist)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_sample(args.workload, 4)
@@ -337,6 +390,21 @@ def main():
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                        "what": "H2D of the initial reference particle records (pinned), K steps each with a D2H "
                                "of the energies, D2H of the final particles"}
+    if ens and "error" in ens:
+        line["ensemble"] = ens
+    elif ens:
+        vb = ens["n"] * ens["K"] / (ens["t_batch"] * 1e-3)
+        vs = ens["n"] * ens["K"] / (ens["t_single"] * 1e-3)
+        line["ensemble"] = {
+            "workload": "64 two-stream/Weibel instances, grids 64x64..256x256, 16-128 ppc/species, FP32",
+            "particles": ens["n"], "steps": ens["K"], "value": vb, "unit": UNIT,
+            "ms_per_step": ens["t_batch"] / ens["K"], "per_instance_value": vs,
+            "per_instance_ms_per_step": ens["t_single"] / ens["K"], "batched_over_per_instance": vb / vs,
+            "autotuned": {"tile_rows": ens["tiles"], "particles_per_thread": 4 * ens["groups"],
+                          "trial_ms_per_step": ens["tune_ms"]},
+            "gpu_launches": {"batched": ens["launches_batch"], "per_instance": ens["launches_single"]},
+            "step_frac_hbm": 96.0 * ens["n"] * ens["K"] / (ens["t_batch"] * 1e-3) / 1e9 / peak,
+            "weibel_gauss_residual_max": ens["gauss"], "status": ens["status"]}
     if cpu:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
                                 "sample": cpu["sample"]}

@@ -242,6 +242,8 @@ int pbpic_batch_set_tiles(pbpic_batch* b, const int32_t* tile_rows, int32_t grou
 int pbpic_batch_get_tiles(const pbpic_batch* b, int32_t* tile_rows, int32_t* groups);
 /* Enqueues nsteps steps of every domain on the batch's stream. */
 int pbpic_batch_step(pbpic_batch* b, int32_t nsteps);
+/* The batch's CUDA stream (a cudaStream_t), for events and ordering. */
+int pbpic_batch_stream(const pbpic_batch* b, void** stream);
 int pbpic_batch_synchronize(pbpic_batch* b);
 /* Times trial_steps steps (real steps of the run: every domain advances) for
  * each candidate tiling (tile rows capped at 16, 32, 64; groups 1, 2), keeps

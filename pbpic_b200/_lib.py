@@ -114,6 +114,7 @@ SIGNATURES = {
     "pbpic_batch_set_tiles": [_P, _P, _I32],
     "pbpic_batch_get_tiles": [_P, _P, _PI32],
     "pbpic_batch_step": [_P, _I32],
+    "pbpic_batch_stream": [_P, ctypes.POINTER(_P)],
     "pbpic_batch_synchronize": [_P],
     "pbpic_batch_autotune": [_P, _I32, _P, _PI32, _PD],
     "pbpic_batch_energies": [_P, _P],

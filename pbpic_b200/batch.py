@@ -76,6 +76,13 @@ class Batch:
     def step(self, nsteps=1):
         L.check(self._lib.pbpic_batch_step(self._b, nsteps))
 
+    @property
+    def stream(self):
+        """The batch's cudaStream_t as an integer (torch.cuda.ExternalStream takes it)."""
+        s = ctypes.c_void_p()
+        L.check(self._lib.pbpic_batch_stream(self._b, ctypes.byref(s)))
+        return s.value or 0
+
     def synchronize(self):
         L.check(self._lib.pbpic_batch_synchronize(self._b))
 

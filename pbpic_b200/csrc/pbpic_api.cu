@@ -1647,6 +1647,13 @@ int pbpic_batch_step(pbpic_batch* b, int32_t nsteps) {
   return batch_step(b, nsteps);
 }
 
+int pbpic_batch_stream(const pbpic_batch* b, void** stream) {
+  TRY(check_batch(b));
+  if (!stream) return fail(PBPIC_EINVAL, "null argument");
+  *stream = (void*)b->stream;
+  return PBPIC_OK;
+}
+
 int pbpic_batch_synchronize(pbpic_batch* b) {
   TRY(check_batch(b));
   CK(cudaStreamSynchronize(b->stream));
