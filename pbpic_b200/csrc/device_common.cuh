@@ -12,11 +12,13 @@ constexpr int NTHREADS = 256;  // threads per block of the particle kernels
 enum { JX = 0, JY = 1, JZ = 2, RHO = 3 };
 
 // Fixed-point scale of the mixed form's current: a deposit value v becomes
-// llrint(v * 2^36). Deposit values are charge * cell-fraction * weight
-// (|v| <= 1.5) or charge * (uz/gamma) * weight (|v| <= 1), so per-node sums of
-// up to 2^26 particles stay below 2^63.
-constexpr float FIX_SCALE = 68719476736.0f;  // 2^36
-constexpr double FIX_INV = 1.0 / 68719476736.0;
+// llrint(v * 2^32) (resolution 2.3e-10, far below the FP32 rounding of the
+// terms). Deposit values are charge * cell-fraction * weight or charge *
+// (uz/gamma) * weight; a single particle's value is below 1 in magnitude (it
+// moves less than a cell per step), so it fits in 33 signed bits, and
+// per-node sums of up to 2^30 particles stay below 2^63.
+constexpr float FIX_SCALE = 4294967296.0f;  // 2^32
+constexpr double FIX_INV = 1.0 / 4294967296.0;
 
 // ---------------------------------------------------------------------------
 // Arithmetic with explicit rounding. Every operation of the particle push

@@ -22,6 +22,16 @@
 // images. Particles outside their tile (array not sorted) add straight to
 // global memory.
 //
+// The window holds int64 fixed-point sums (mixed form), and 64-bit shared
+// atomics are slow. A crossing particle's four second-segment values (each
+// below 2^32 in fixed point) therefore go to a separate pair of 32-bit
+// windows: the low 17 bits to an unsigned sum and the rest (signed) to a
+// second sum, both with native 32-bit atomics. With at most 32767 particles
+// in the tile neither sum can overflow (32767 * (2^17 - 1) < 2^32 and
+// 32767 * 2^15 < 2^31); larger tiles use the 64-bit window. Integer sums do
+// not depend on the order of the atomics, so the result is the same bits
+// either way.
+//
 // With HIST the kernel also counts the new cells of its particles in the
 // tile's window (the 3x3 neighbourhood of the tile), the first half of the
 // fused counting sort (kernels_sort.cuh).
@@ -368,6 +378,14 @@ __device__ __forceinline__ void acc_add(long long* p, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
 }
 
+// A crossing particle's value v (|v| < 2^32, fixed point) into the split
+// 32-bit windows: v = hi * 2^17 + lo with 0 <= lo < 2^17.
+__device__ __forceinline__ void cross_add(unsigned* lo, int* hi, int idx, long long v) {
+  atomicAdd(&lo[idx], (unsigned)(v & 0x1ffff));
+  atomicAdd(&hi[idx], (int)(v >> 17));
+}
+__device__ __forceinline__ void cross_add(unsigned*, int*, int, double) {}
+
 template <class T, bool MIXED>
 __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::type to_acc(T v) {
   if constexpr (MIXED) {
@@ -453,15 +471,23 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   const int TY = a.tile_rows, WR = TY + 3, NB = 3 * (TY + 2);
   Acc* win = reinterpret_cast<Acc*>(smem_raw);
   int* hist = reinterpret_cast<int*>(win + 16 * WR);
+  unsigned* clo = reinterpret_cast<unsigned*>(hist + NB);  // crossers: jx, jy planes (8 * WR)
+  int* chi = reinterpret_cast<int*>(clo + 8 * WR);
   const int ixt = t / a.tiles_per_col;
   const int y0 = (t - ixt * a.tiles_per_col) * TY;
   const int y1 = min(y0 + TY, a.my);
   for (int e = threadIdx.x; e < 16 * WR; e += blockDim.x) win[e] = Acc(0);
+  if (MIXED)
+    for (int e = threadIdx.x; e < 8 * WR; e += blockDim.x) {
+      clo[e] = 0u;
+      chi[e] = 0;
+    }
   if (HIST)
     for (int e = threadIdx.x; e < NB; e += blockDim.x) hist[e] = 0;
   __syncthreads();
   Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
+  const bool split = MIXED && pend - pbeg <= 32767;  // crossers to the 32-bit windows
   const unsigned lane = lane_id();
   const int w = threadIdx.x >> 5;
   // this lane's entry of the stencil when it deposits a run's sum
@@ -583,10 +609,18 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           acc[16] += o.e[15];
           if (cross) {  // second zig-zag segment, attached to the new cell
             const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
-            acc_add(&win[(JX * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[2]));
-            acc_add(&win[(JX * 4 + wx) * WR + wy + 1], to_acc<T, MIXED>(o.e[3]));
-            acc_add(&win[(JY * 4 + wx) * WR + wy], to_acc<T, MIXED>(o.e[6]));
-            acc_add(&win[(JY * 4 + wx + 1) * WR + wy], to_acc<T, MIXED>(o.e[7]));
+            const int b0 = (JX * 4 + wx) * WR + wy, b1 = (JY * 4 + wx) * WR + wy;
+            if (split) {
+              cross_add(clo, chi, b0, to_acc<T, MIXED>(o.e[2]));
+              cross_add(clo, chi, b0 + 1, to_acc<T, MIXED>(o.e[3]));
+              cross_add(clo, chi, b1, to_acc<T, MIXED>(o.e[6]));
+              cross_add(clo, chi, b1 + WR, to_acc<T, MIXED>(o.e[7]));
+            } else {
+              acc_add(&win[b0], to_acc<T, MIXED>(o.e[2]));
+              acc_add(&win[b0 + 1], to_acc<T, MIXED>(o.e[3]));
+              acc_add(&win[b1], to_acc<T, MIXED>(o.e[6]));
+              acc_add(&win[b1 + WR], to_acc<T, MIXED>(o.e[7]));
+            }
           }
         } else {
           status |= 4;
@@ -665,7 +699,8 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   __syncthreads();
   // Fold the window into the global current.
   for (int e = threadIdx.x; e < 16 * WR; e += blockDim.x) {
-    const Acc val = win[e];
+    Acc val = win[e];
+    if (MIXED && e < 8 * WR) val += (Acc)(((long long)chi[e] << 17) + (long long)clo[e]);
     if (val == Acc(0)) continue;
     const int c = e / (4 * WR);
     const int r = e - c * 4 * WR;

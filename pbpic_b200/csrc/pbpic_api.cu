@@ -192,6 +192,14 @@ int dalloc(pbpic_handle* h, P** p, size_t bytes) {
 
 int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
 
+// Dynamic shared memory of k_push: the tile's current window (16 x (ty+3)
+// 8-byte accumulators), the new-cell histogram (3 x (ty+2) int) and, in the
+// mixed form, the crossers' split 32-bit windows (2 x 8 x (ty+3)). With the
+// static part this stays below the 48 KB a launch gets without opting in.
+size_t push_smem_bytes(int ty, bool mixed) {
+  return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (mixed ? (size_t)16 * (ty + 3) * 4 : 0);
+}
+
 int ensure_staging(pbpic_handle* h, size_t bytes) {
   if (h->staging_bytes >= bytes) return PBPIC_OK;
   if (h->staging) {
@@ -381,7 +389,7 @@ int do_push(pbpic_handle* h) {
   TRY(ensure_hist(h, h->itime + 2));
   CK(cudaMemsetAsync(h->jacc, 0, (size_t)4 * plane_elems(h) * 8, s));
   PushParams<T> p = push_params<T, MIXED>(h);
-  const size_t smem = (size_t)16 * (h->TY + 3) * 8 + (size_t)h->nb * 4;
+  const size_t smem = push_smem_bytes(h->TY, MIXED);
   const bool hist = h->sorted && h->fused_ok;
   if (hist) k_push<T, MIXED, true><<<h->ntiles, NTHREADS, smem, s>>>(p);
   else k_push<T, MIXED, false><<<h->ntiles, NTHREADS, smem, s>>>(p);
@@ -1297,7 +1305,7 @@ int batch_layout(pbpic_batch* b) {
       const int rows = std::min(h->TY, h->cfg.my - y0);
       items.push_back({rows * ppc, d, t});
     }
-    smem = std::max(smem, (size_t)16 * (h->TY + 3) * 8 + (size_t)h->nb * 4);
+    smem = std::max(smem, push_smem_bytes(h->TY, true));
     maxcells = std::max<int64_t>(maxcells, (int64_t)h->ncells + 1);
     maxbins = std::max<int64_t>(maxbins, (int64_t)h->ntiles * h->nb);
     maxtiles = std::max<int64_t>(maxtiles, (int64_t)h->ntiles + 1);

@@ -278,7 +278,8 @@ def test_bad_particle_records_are_rejected(gpu_lib, oracle_mod):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("ybc,mx,my,ty", [(0, 16, 12, 0), (0, 9, 20, 6), (1, 16, 12, 0), (1, 7, 13, 5), (1, 8, 40, 64)])
+@pytest.mark.parametrize("ybc,mx,my,ty", [(0, 16, 12, 0), (0, 9, 20, 6), (1, 16, 12, 0), (1, 7, 13, 5), (1, 8, 40, 64),
+                                         (1, 5, 70, 0), (0, 4, 80, 0)])
 def test_fused_sort_is_the_stable_sort(gpu_lib, oracle_mod, precision, ybc, mx, my, ty):
     """After a push on a sorted array, the counting sort from the push's
     per-tile histograms gives exactly the stable sort by cell (array order
