@@ -51,6 +51,7 @@ extern "C" {
 #define PBPIC_STATUS_CELL_JUMP 1 /* a particle moved more than one cell in a step (pic2d.f90:1008-1023 assumes at most one) */
 #define PBPIC_STATUS_NAN 2       /* a momentum became NaN or infinite */
 #define PBPIC_STATUS_UNSORTED 4  /* a push met a particle outside its tile (informational) */
+#define PBPIC_STATUS_COPY_TIMEOUT 16 /* a bulk copy into shared memory did not complete within 2 s (the step's results are invalid) */
 
 typedef struct pbpic_config {
   int32_t mx, my;      /* cells in x and y (nx, ny of pic2d.f90:12; one domain) */

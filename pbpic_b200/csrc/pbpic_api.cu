@@ -401,6 +401,20 @@ int do_push(pbpic_handle* h) {
   return PBPIC_OK;
 }
 
+// The staged scatter takes more than the default 48 KB of dynamic shared
+// memory; the attribute is set once per process (one device per process).
+template <class T>
+int staged_scatter_attr() {
+  static std::once_flag once;
+  static cudaError_t err = cudaSuccess;
+  std::call_once(once, [] {
+    err = cudaFuncSetAttribute(k_fused_scatter_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)StageLayout<T>::BYTES);
+  });
+  if (err != cudaSuccess) return fail(PBPIC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
+  return PBPIC_OK;
+}
+
 // Counting sort from the per-tile histograms of the last push (kernels_sort.cuh).
 template <class T, bool MIXED>
 int do_fused_sort(pbpic_handle* h) {
@@ -449,8 +463,9 @@ int do_fused_sort(pbpic_handle* h) {
   sp.uzo = P<T>(h, o, 4);
   sp.pido = h->pid[o];
   if (n > 0) {
-    k_fused_scatter<T><<<h->ntiles, 256, 0, s>>>(sp);
-    CKLAUNCH("k_fused_scatter");
+    TRY(staged_scatter_attr<T>());
+    k_fused_scatter_staged<T><<<h->ntiles, 256, StageLayout<T>::BYTES, s>>>(sp, h->status);
+    CKLAUNCH("k_fused_scatter_staged");
     h->cur = o;
   }
   k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, h->cfg.my,
@@ -765,9 +780,10 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
     if (r == PBPIC_OK) r = dalloc(h, p, bytes);
   };
   for (int b = 0; b < 2; ++b) {
-    A(&h->cell[b], capn * 4);
-    for (int k = 0; k < 5; ++k) A(&h->comp[b][k], capn * h->tsz);
-    if (c.track_pid) A(&h->pid[b], capn * 4);
+    // particle arrays carry 16 elements of padding: bulk copies read whole 16-byte units
+    A(&h->cell[b], (capn + 16) * 4);
+    for (int k = 0; k < 5; ++k) A(&h->comp[b][k], (capn + 16) * h->tsz);
+    if (c.track_pid) A(&h->pid[b], (capn + 16) * 4);
     A(&h->keys[b], capn * 4);
     A(&h->vals[b], capn * 4);
   }
