@@ -109,6 +109,12 @@ struct Pushed {
   T dx, dy, ux, uy, uz;  // new state (after reflection)
   int dcx, dcy, di, dj;  // cell steps and jz quadrant
   T e[16];               // deposit terms: jx 4, jy 4, jz 4, rho 4
+  // mixed form, cell-stencil form of the same deposit: jx at (0,0), (0,1) is
+  // ja*(1-jw), ja*jw (first segment only for a crossing particle, the whole
+  // move otherwise), jy at (0,0), (1,0) is jb*(1-jv), jb*jv; jz is quz times
+  // the outer product of the x and y midpoint weights (1-zdx at 0, zdx at
+  // di; 1-zdy at 0, zdy at dj)
+  T ja, jw, jb, jv, quz, zdx, zdy;
   T ke;                  // kinetic energy (gamma - 1) ms
   int status;
 };
@@ -218,6 +224,11 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
     o.e[5] = A::mul(fy1, wx1);        // jy (1, 0)
     o.e[6] = A::mad(-fy2, wx2, fy2);  // jy (dcx, dcy)
     o.e[7] = A::mul(fy2, wx2);        // jy (dcx+1, dcy)
+    const bool cr = dcx != 0 || dcy != 0;
+    o.ja = cr ? fx1 : A::mul(qx, A::sub(xe, xs));
+    o.jw = cr ? wy1 : jm;
+    o.jb = cr ? fy1 : A::mul(qy, A::sub(ye, ys));
+    o.jv = cr ? wx1 : im;
   } else {
     im = A::mul(A::add(A::add(A::add(fdcx, px), dx2), one), half);
     jm = A::mul(A::add(A::add(A::add(fdcy, py), dy2), one), half);
@@ -250,6 +261,9 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
     const T z3 = A::sub(djmid, z1);
     const T z4 = A::sub(A::sub(A::sub(one, z1), z2), z3);
     const T quz = A::mul(qq, vz);
+    o.quz = quz;
+    o.zdx = dimid;
+    o.zdy = djmid;
     o.e[8] = A::mul(quz, z4);   // jz (0, 0)
     o.e[9] = A::mul(quz, z2);   // jz (di, 0)
     o.e[10] = A::mul(quz, z3);  // jz (0, dj)
@@ -587,22 +601,42 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
             }
             acc_key = key;
           }
-          acc[0] += cross ? o.e[0] : o.e[0] + o.e[2];
-          acc[1] += cross ? o.e[1] : o.e[1] + o.e[3];
-          acc[2] += cross ? o.e[4] : o.e[4] + o.e[6];
-          acc[3] += cross ? o.e[5] : o.e[5] + o.e[7];
-          // jz: (0,0) <- e8, (di,0) <- e9, (0,dj) <- e10, (di,dj) <- e11 with di, dj = +-1
-          const T zxm = o.di < 0 ? T(1) : T(0), zxp = o.di > 0 ? T(1) : T(0);
-          const T zym = o.dj < 0 ? T(1) : T(0), zyp = o.dj > 0 ? T(1) : T(0);
-          acc[4 + 0] += zxm * zym * o.e[11];
-          acc[4 + 1] += zxm * o.e[9];
-          acc[4 + 2] += zxm * zyp * o.e[11];
-          acc[4 + 3] += zym * o.e[10];
-          acc[4 + 4] += o.e[8];
-          acc[4 + 5] += zyp * o.e[10];
-          acc[4 + 6] += zxp * zym * o.e[11];
-          acc[4 + 7] += zxp * o.e[9];
-          acc[4 + 8] += zxp * zyp * o.e[11];
+          if constexpr (MIXED) {
+            acc[0] = __fadd_rn(acc[0], __fmaf_rn(-o.ja, o.jw, o.ja));
+            acc[1] = __fmaf_rn(o.ja, o.jw, acc[1]);
+            acc[2] = __fadd_rn(acc[2], __fmaf_rn(-o.jb, o.jv, o.jb));
+            acc[3] = __fmaf_rn(o.jb, o.jv, acc[3]);
+            // jz: outer product of the x weights (x = -1, 0, 1) and y weights
+            const T qs = __fmul_rn(o.quz, o.zdx), q0 = __fsub_rn(o.quz, qs);
+            const T qxm = o.di < 0 ? qs : T(0), qxp = o.di > 0 ? qs : T(0);
+            const T ym = o.dj < 0 ? o.zdy : T(0), yp = o.dj > 0 ? o.zdy : T(0), y0 = __fsub_rn(T(1), o.zdy);
+            acc[4 + 0] = __fmaf_rn(qxm, ym, acc[4 + 0]);
+            acc[4 + 1] = __fmaf_rn(qxm, y0, acc[4 + 1]);
+            acc[4 + 2] = __fmaf_rn(qxm, yp, acc[4 + 2]);
+            acc[4 + 3] = __fmaf_rn(q0, ym, acc[4 + 3]);
+            acc[4 + 4] = __fmaf_rn(q0, y0, acc[4 + 4]);
+            acc[4 + 5] = __fmaf_rn(q0, yp, acc[4 + 5]);
+            acc[4 + 6] = __fmaf_rn(qxp, ym, acc[4 + 6]);
+            acc[4 + 7] = __fmaf_rn(qxp, y0, acc[4 + 7]);
+            acc[4 + 8] = __fmaf_rn(qxp, yp, acc[4 + 8]);
+          } else {
+            acc[0] += cross ? o.e[0] : o.e[0] + o.e[2];
+            acc[1] += cross ? o.e[1] : o.e[1] + o.e[3];
+            acc[2] += cross ? o.e[4] : o.e[4] + o.e[6];
+            acc[3] += cross ? o.e[5] : o.e[5] + o.e[7];
+            // jz: (0,0) <- e8, (di,0) <- e9, (0,dj) <- e10, (di,dj) <- e11 with di, dj = +-1
+            const T zxm = o.di < 0 ? T(1) : T(0), zxp = o.di > 0 ? T(1) : T(0);
+            const T zym = o.dj < 0 ? T(1) : T(0), zyp = o.dj > 0 ? T(1) : T(0);
+            acc[4 + 0] += zxm * zym * o.e[11];
+            acc[4 + 1] += zxm * o.e[9];
+            acc[4 + 2] += zxm * zyp * o.e[11];
+            acc[4 + 3] += zym * o.e[10];
+            acc[4 + 4] += o.e[8];
+            acc[4 + 5] += zyp * o.e[10];
+            acc[4 + 6] += zxp * zym * o.e[11];
+            acc[4 + 7] += zxp * o.e[9];
+            acc[4 + 8] += zxp * zyp * o.e[11];
+          }
           acc[13] += o.e[12];
           acc[14] += o.e[13];
           acc[15] += o.e[14];

@@ -449,15 +449,19 @@ __global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
 
 // ------------------------------------------- scatter with bulk-copy staging
 // The same stable scatter, with each chunk's particle arrays brought into
-// shared memory by the bulk-copy (TMA) engine, cp.async.bulk, double
-// buffered: while the block ranks and writes chunk k, the copies of chunk
-// k+1 are in flight, so the DRAM stream does not wait on the ranking. Copies
+// shared memory by the bulk-copy (TMA) engine, cp.async.bulk, in a ring of
+// SB_NS buffers: while the block ranks and writes chunk k, the copies of
+// chunks k+1 .. k+SB_NS-1 are in flight, so the DRAM stream does not wait on
+// the ranking. Copies
 // start on 16-byte boundaries (the chunk start rounded down, its end rounded
 // up; particle arrays carry 16 elements of padding) and complete on an
 // mbarrier. Every wait is bounded (2 s of %globaltimer): on a timeout the
 // block sets status bit 16, waits (bounded again) for its copies still in
 // flight and returns.
-constexpr int SB_IPT = 4, SB_CH = 256 * SB_IPT;
+#ifndef PBPIC_SCATTER_STAGES
+#define PBPIC_SCATTER_STAGES 3
+#endif
+constexpr int SB_IPT = 4, SB_CH = 256 * SB_IPT, SB_NS = PBPIC_SCATTER_STAGES;
 
 template <class T>
 struct StageLayout {
@@ -466,13 +470,13 @@ struct StageLayout {
   static constexpr int N4 = SB_CH + 2 * P4;        // capacity of a 4-byte array buffer
   static constexpr int NT = SB_CH + 2 * PT;
   static constexpr size_t BUF = (size_t)2 * N4 * 4 + (size_t)5 * NT * sizeof(T);  // cell, pid, 5 x T
-  static constexpr size_t BYTES = 2 * BUF;         // double buffer
+  static constexpr size_t BYTES = SB_NS * BUF;     // ring of SB_NS buffers
 };
 
 struct StageSmem {
   int32_t cnt[8][SC_MAXNB];
   int32_t run[SC_MAXNB], sbase[SC_MAXNB];
-  unsigned long long bar[2];
+  unsigned long long bar[SB_NS];
   int ok;
 };
 
@@ -560,7 +564,7 @@ __device__ __forceinline__ void stage_issue(const ScatterParams<T>& a, unsigned 
 
 template <class T>
 __device__ __forceinline__ void scatter_tile_staged(const ScatterParams<T>& a, const int t, StageSmem& sm,
-                                                    unsigned char* stage, unsigned (&phase)[2], int* status) {
+                                                    unsigned char* stage, unsigned& phase, int* status) {
   using L = StageLayout<T>;
   int32_t(&cnt)[8][SC_MAXNB] = sm.cnt;
   const int ixt = t / a.tpc, y0 = (t - ixt * a.tpc) * a.ty, y1 = min(y0 + a.ty, a.my);
@@ -572,26 +576,30 @@ __device__ __forceinline__ void scatter_tile_staged(const ScatterParams<T>& a, c
     sm.run[b] = 0;
     sm.sbase[b] = a.base[(int64_t)t * a.nb + b];
   }
+  // `phase` holds the parity bit of each ring buffer's next completion
   if (threadIdx.x == 0)
-    for (int k = 0; k < 2 && k < nchunks; ++k)
+    for (int k = 0; k < SB_NS && k < nchunks; ++k)
       stage_issue(a, stage, k, pbeg + k * SB_CH, min(pbeg + (k + 1) * SB_CH, pend), &sm.bar[k]);
   for (int k = 0; k < nchunks; ++k) {
-    const int buf = k & 1;
+    const int buf = k % SB_NS;
+    const unsigned par = (phase >> buf) & 1u;
     const int c0 = pbeg + k * SB_CH, c1 = min(c0 + SB_CH, pend);
     for (int e = threadIdx.x; e < 8 * SC_MAXNB; e += blockDim.x) (&cnt[0][0])[e] = 0;
-    if (threadIdx.x == 0) sm.ok = mbar_wait_bounded(&sm.bar[buf], phase[buf]) ? 1 : 0;
+    if (threadIdx.x == 0) sm.ok = mbar_wait_bounded(&sm.bar[buf], par) ? 1 : 0;
     __syncthreads();
     if (!sm.ok) {  // the copy did not arrive: flag, drain what is in flight, give up the tile
       if (threadIdx.x == 0) {
         atomicOr(status, 16);
-        mbar_wait_bounded(&sm.bar[buf], phase[buf]);
-        if (k + 1 < nchunks) mbar_wait_bounded(&sm.bar[buf ^ 1], phase[buf ^ 1]);
+        for (int j = 0; j < SB_NS && k + j < nchunks; ++j) {
+          const int bj = (k + j) % SB_NS;
+          mbar_wait_bounded(&sm.bar[bj], (phase >> bj) & 1u);
+        }
       }
       __syncthreads();
       return;
     }
-    mbar_wait_bounded(&sm.bar[buf], phase[buf]);  // completed: every thread acquires the copied data
-    phase[buf] ^= 1u;
+    mbar_wait_bounded(&sm.bar[buf], par);  // completed: every thread acquires the copied data
+    phase ^= 1u << buf;
     const StageView<T> s = stage_view<T>(stage, buf);
     const int s4 = c0 - (c0 & ~(L::P4 - 1)), sT = c0 - (c0 & ~(L::PT - 1));
     int bin[SB_IPT], pos[SB_IPT];
@@ -639,8 +647,8 @@ __device__ __forceinline__ void scatter_tile_staged(const ScatterParams<T>& a, c
       }
     }
     __syncthreads();  // buffer `buf` is free again
-    if (threadIdx.x == 0 && k + 2 < nchunks)
-      stage_issue(a, stage, buf, pbeg + (k + 2) * SB_CH, min(pbeg + (k + 3) * SB_CH, pend), &sm.bar[buf]);
+    if (threadIdx.x == 0 && k + SB_NS < nchunks)
+      stage_issue(a, stage, buf, pbeg + (k + SB_NS) * SB_CH, min(pbeg + (k + SB_NS + 1) * SB_CH, pend), &sm.bar[buf]);
   }
 }
 
@@ -649,12 +657,11 @@ __global__ void __launch_bounds__(256) k_fused_scatter_staged(ScatterParams<T> a
   extern __shared__ __align__(128) unsigned char stage[];
   __shared__ StageSmem sm;
   if (threadIdx.x == 0) {
-    mbar_init(&sm.bar[0], 1);
-    mbar_init(&sm.bar[1], 1);
+    for (int j = 0; j < SB_NS; ++j) mbar_init(&sm.bar[j], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  unsigned phase[2] = {0u, 0u};
+  unsigned phase = 0u;
   scatter_tile_staged(a, blockIdx.x, sm, stage, phase, status);
 }
 
