@@ -214,6 +214,21 @@ int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
 int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t ncells,
                                     int32_t* perm_dev, int32_t* counts_dev, void* stream);
 
+/* --------------------------------------------------------- dump / restart */
+/* Writes the handle's state to directory `dir` (created if missing) as .npy
+ * files named like the datasets of the reference's particle and field dumps
+ * (particlesinfo / fieldsinfo, pic2d.f90:1358-1380, 1625-1644; HDF5 there):
+ * particles/{dx,dy,ux,uy,uz,grid,q[,pid]}, fields/{ex,ey,ez,bx,by,bz} and
+ * fields/{jx,jy,jz,rho} (mx x (my+1)), totene (itime+1 x 4) and state.json.
+ * Values keep the handle's precision, so pbpic_restart reproduces the state
+ * exactly. */
+int pbpic_dump(pbpic_handle* h, const char* dir);
+/* Loads a dump into a handle created with the same mx, my, ybc and precision
+ * and enough capacity, sets its time step and energy history, and sorts the
+ * particles (stable, so a dump taken right after a sort continues bit for
+ * bit). */
+int pbpic_restart(pbpic_handle* h, const char* dir);
+
 /* ------------------------------------------------------------ batched form */
 /* Many independent domains of uneven grid size and particle count advanced
  * together. Every phase of a step runs once for all domains: persistent

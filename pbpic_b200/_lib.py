@@ -107,6 +107,8 @@ SIGNATURES = {
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],
     "pbpic_kernel_launches": [_PI64],
     "pbpic_counting_sort_keys_static": [_P, _I64, _I32, _P, _P, _P],
+    "pbpic_dump": [_P, ctypes.c_char_p],
+    "pbpic_restart": [_P, ctypes.c_char_p],
     "pbpic_batch_create": [ctypes.POINTER(Config), ctypes.POINTER(Loader), _I32, ctypes.POINTER(_P)],
     "pbpic_batch_destroy": [_P],
     "pbpic_batch_num_domains": [_P, _PI32],

@@ -4,6 +4,8 @@
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+#include <errno.h>
+#include <sys/stat.h>
 
 #include <algorithm>
 #include <atomic>
@@ -19,6 +21,7 @@
 #include "kernels_misc.cuh"
 #include "kernels_push.cuh"
 #include "kernels_sort.cuh"
+#include "npy_io.h"
 #include "pic_common.h"
 #include "pic_fields_init.h"
 
@@ -1739,6 +1742,166 @@ int pbpic_batch_energies(pbpic_batch* b, double* out) {
   }
   CK(cudaStreamSynchronize(b->stream));
   return PBPIC_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ dump / restart
+// The state of a handle as a directory of .npy files named like the datasets
+// of the reference's HDF5 dumps (particlesinfo, pic2d.f90:1358-1380, and
+// fieldsinfo, pic2d.f90:1625-1644): particles/{dx,dy,ux,uy,uz,grid,q,pid},
+// fields/{ex,ey,ez,bx,by,bz} (mx x (my+1), the layout of pbpic_store_fields),
+// fields/{jx,jy,jz,rho} (the last push's current, as pbpic_store_denjr),
+// totene (itime+1 x 4) and state.json (the run parameters, itime and counts).
+// Particle and field values keep the handle's precision (<f4 mixed, <f8
+// plain), so a restart reproduces the state exactly. HDF5 itself is not used.
+namespace {
+
+bool make_dir(const std::string& d) { return mkdir(d.c_str(), 0755) == 0 || errno == EEXIST; }
+
+template <class T>
+const char* npy_descr() {
+  return sizeof(T) == 4 ? "<f4" : "<f8";
+}
+
+template <class T, bool MIXED>
+int do_dump(pbpic_handle* h, const std::string& dir) {
+  if (!make_dir(dir) || !make_dir(dir + "/particles") || !make_dir(dir + "/fields"))
+    return fail(PBPIC_EINVAL, "cannot create the dump directory " + dir);
+  const int64_t n = h->n;
+  std::vector<pbpic_particle_f64> rec((size_t)std::max<int64_t>(n, 1));
+  int64_t got = 0;
+  TRY(pbpic_store_particles_f64(h, rec.data(), n, &got));
+  std::vector<T> v((size_t)std::max<int64_t>(n, 1));
+  std::vector<int32_t> iv((size_t)std::max<int64_t>(n, 1));
+  const char* names[5] = {"dx", "dy", "ux", "uy", "uz"};
+  for (int c = 0; c < 5; ++c) {
+    for (int64_t i = 0; i < n; ++i) {
+      const pbpic_particle_f64& r = rec[i];
+      const double x = c == 0 ? r.dx : c == 1 ? r.dy : c == 2 ? r.ux : c == 3 ? r.uy : r.uz;
+      v[i] = (T)x;  // exact: the values are the device's T values
+    }
+    if (!npyio::write(dir + "/particles/" + names[c] + ".npy", npy_descr<T>(), {n}, v.data(), (size_t)n * sizeof(T)))
+      return fail(PBPIC_EINVAL, "cannot write " + dir + "/particles");
+  }
+  const char* inames[3] = {"grid", "q", "pid"};
+  for (int c = 0; c < 3; ++c) {
+    if (c == 2 && !h->cfg.track_pid) continue;
+    for (int64_t i = 0; i < n; ++i) iv[i] = c == 0 ? rec[i].grid : c == 1 ? rec[i].q : rec[i].pid;
+    if (!npyio::write(dir + "/particles/" + inames[c] + ".npy", "<i4", {n}, iv.data(), (size_t)n * 4))
+      return fail(PBPIC_EINVAL, "cannot write " + dir + "/particles");
+  }
+  const int64_t pe = plane_elems(h);
+  std::vector<double> f6((size_t)(6 * pe)), j4((size_t)(4 * pe));
+  TRY((do_store_fields<T, MIXED>(h, f6.data())));
+  TRY(do_store_denjr(h, j4.data()));
+  const char* fnames[6] = {"ex", "ey", "ez", "bx", "by", "bz"};
+  std::vector<T> plane((size_t)pe);
+  for (int c = 0; c < 6; ++c) {
+    for (int64_t k = 0; k < pe; ++k) plane[k] = (T)f6[(size_t)c * pe + k];
+    if (!npyio::write(dir + "/fields/" + fnames[c] + ".npy", npy_descr<T>(), {h->cfg.mx, h->S}, plane.data(),
+                      (size_t)pe * sizeof(T)))
+      return fail(PBPIC_EINVAL, "cannot write " + dir + "/fields");
+  }
+  const char* jnames[4] = {"jx", "jy", "jz", "rho"};
+  for (int c = 0; c < 4; ++c)
+    if (!npyio::write(dir + "/fields/" + jnames[c] + ".npy", "<f8", {h->cfg.mx, h->S}, j4.data() + (size_t)c * pe,
+                      (size_t)pe * 8))
+      return fail(PBPIC_EINVAL, "cannot write " + dir + "/fields");
+  const int rows = h->itime + 1;
+  std::vector<double> hist((size_t)rows * 4);
+  CK(cudaMemcpyAsync(hist.data(), h->hist, hist.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (!npyio::write(dir + "/totene.npy", "<f8", {rows, 4}, hist.data(), hist.size() * 8))
+    return fail(PBPIC_EINVAL, "cannot write " + dir + "/totene.npy");
+  const pbpic_config& c = h->cfg;
+  if (!npyio::write_numbers(dir + "/state.json",
+                            {{"format", 1}, {"mx", c.mx}, {"my", c.my}, {"dx", c.dx}, {"dy", c.dy}, {"dt", c.dt},
+                             {"cva", c.cva}, {"mime", c.mime}, {"in0", c.in0}, {"ybc", c.ybc},
+                             {"precision", c.precision}, {"compat", c.compat}, {"track_pid", c.track_pid},
+                             {"itime", h->itime}, {"particles", (double)n}}))
+    return fail(PBPIC_EINVAL, "cannot write " + dir + "/state.json");
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_restart(pbpic_handle* h, const std::string& dir) {
+  std::map<std::string, double> st;
+  if (!npyio::read_numbers(dir + "/state.json", &st) || !st.count("itime") || !st.count("particles"))
+    return fail(PBPIC_EINVAL, "cannot read " + dir + "/state.json");
+  const pbpic_config& c = h->cfg;
+  if ((int)st["mx"] != c.mx || (int)st["my"] != c.my || (int)st["ybc"] != c.ybc || (int)st["precision"] != c.precision)
+    return fail(PBPIC_EINVAL, "the dump's mx, my, ybc or precision differ from the handle's");
+  const int64_t n = (int64_t)st["particles"];
+  const int itime = (int)st["itime"];
+  if (n > h->cap) return fail(PBPIC_ECAPACITY, "the dump holds more particles than the handle's capacity");
+  auto load = [&](const std::string& name, const char* descr, int64_t count, npyio::Array* a) -> int {
+    const std::string err = npyio::read(dir + "/" + name + ".npy", a);
+    if (!err.empty()) return fail(PBPIC_EINVAL, err);
+    if (a->descr != descr || a->count() != count) return fail(PBPIC_EINVAL, dir + "/" + name + ".npy: unexpected dtype or shape");
+    return PBPIC_OK;
+  };
+  std::vector<pbpic_particle_f64> rec((size_t)std::max<int64_t>(n, 1));
+  const char* names[5] = {"dx", "dy", "ux", "uy", "uz"};
+  for (int k = 0; k < 5; ++k) {
+    npyio::Array a;
+    TRY(load(std::string("particles/") + names[k], npy_descr<T>(), n, &a));
+    const T* p = reinterpret_cast<const T*>(a.data.data());
+    for (int64_t i = 0; i < n; ++i) {
+      double* dst = k == 0 ? &rec[i].dx : k == 1 ? &rec[i].dy : k == 2 ? &rec[i].ux : k == 3 ? &rec[i].uy : &rec[i].uz;
+      *dst = (double)p[i];
+    }
+  }
+  const char* inames[3] = {"grid", "q", "pid"};
+  for (int k = 0; k < 3; ++k) {
+    npyio::Array a;
+    if (k == 2) {
+      for (int64_t i = 0; i < n; ++i) rec[i].pid = 0;
+      if (!c.track_pid) continue;
+      FILE* f = fopen((dir + "/particles/pid.npy").c_str(), "rb");
+      if (!f) continue;  // dumped without particle ids
+      fclose(f);
+    }
+    TRY(load(std::string("particles/") + inames[k], "<i4", n, &a));
+    const int32_t* p = reinterpret_cast<const int32_t*>(a.data.data());
+    for (int64_t i = 0; i < n; ++i) (k == 0 ? rec[i].grid : k == 1 ? rec[i].q : rec[i].pid) = p[i];
+  }
+  for (int64_t i = 0; i < n; ++i) rec[i].pad = 0;
+  npyio::Array hist;
+  TRY(load("totene", "<f8", (int64_t)(itime + 1) * 4, &hist));
+  const int64_t pe = plane_elems(h);
+  std::vector<double> f6((size_t)(6 * pe));
+  const char* fnames[6] = {"ex", "ey", "ez", "bx", "by", "bz"};
+  for (int k = 0; k < 6; ++k) {
+    npyio::Array a;
+    TRY(load(std::string("fields/") + fnames[k], npy_descr<T>(), pe, &a));
+    const T* p = reinterpret_cast<const T*>(a.data.data());
+    for (int64_t i = 0; i < pe; ++i) f6[(size_t)k * pe + i] = (double)p[i];
+  }
+  TRY(pbpic_load_particles_f64(h, rec.data(), n));
+  h->itime = itime;
+  TRY(ensure_hist(h, itime + 2));
+  CK(cudaMemcpyAsync(h->hist, hist.data.data(), hist.data.size(), cudaMemcpyHostToDevice, h->stream));
+  TRY((do_load_fields<T, MIXED>(h, f6.data())));
+  TRY((do_sort<T, MIXED>(h)));
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbpic_dump(pbpic_handle* h, const char* dir) {
+  TRY(check_handle(h));
+  if (!dir) return fail(PBPIC_EINVAL, "null directory");
+  return DISPATCH(h, do_dump, h, std::string(dir));
+}
+
+int pbpic_restart(pbpic_handle* h, const char* dir) {
+  TRY(check_handle(h));
+  if (!dir) return fail(PBPIC_EINVAL, "null directory");
+  return DISPATCH(h, do_restart, h, std::string(dir));
 }
 
 }  // extern "C"

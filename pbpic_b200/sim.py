@@ -144,6 +144,15 @@ class Simulation:
     def synchronize(self):
         L.check(self._lib.pbpic_synchronize(self._h))
 
+    # ---------------------------------------------------------- dump / restart
+    def dump(self, directory):
+        """Write the state as .npy files named like the reference's dump datasets."""
+        L.check(self._lib.pbpic_dump(self._h, str(directory).encode()))
+
+    def restart(self, directory):
+        """Load a dump written by dump() (same grid, boundary and precision)."""
+        L.check(self._lib.pbpic_restart(self._h, str(directory).encode()))
+
     # ------------------------------------------------------------- diagnostics
     def energies(self):
         a = np.zeros(4)
