@@ -185,6 +185,17 @@ int pbpic_cell_counts(pbpic_handle* h, int32_t* counts);
 int pbpic_gauss_residual(pbpic_handle* h, double* out);
 /* Reconnected flux: half the sum of |By| along the node row my/2 times dx. */
 int pbpic_reconnected_flux(pbpic_handle* h, double* out);
+/* Optional field filters, off by default as in the reference, which defines
+ * them and comments out their call after the E update (pic2d.f90:754-755):
+ * Marder divergence cleaning (divergenceclean, pic2d.f90:867-886; marder_d
+ * is its constant, <= 0 selects the reference's 0.001) and the Cherenkov
+ * filter (suppresscerenkov, pic2d.f90:889-907; tau = cerenkov_tau * dt,
+ * <= 0 selects the reference's 0.125). Periodic y only. Not applied by the
+ * batched form. */
+#define PBPIC_FILTER_MARDER 1
+#define PBPIC_FILTER_CERENKOV 2
+int pbpic_set_field_filters(pbpic_handle* h, int32_t flags, double marder_d, double cerenkov_tau);
+
 /* Device status bits (PBPIC_STATUS_*) accumulated since the last call; clears them. */
 int pbpic_status(pbpic_handle* h, int32_t* bits);
 /* Number of CUDA kernels this library has launched in the process (all handles). */

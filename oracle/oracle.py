@@ -68,6 +68,7 @@ def lib():
         for f in ("orc_pusher", "orc_fieldsolver"):
             getattr(L, f).argtypes = [P]
         L.orc_countingsort.argtypes = [P, P]
+        L.orc_set_filters.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         L.orc_omp_pusher.argtypes = [P, ctypes.c_int]
         L.orc_omp_countingsort.argtypes = [P, ctypes.c_int]
         L.orc_omp_max_threads.restype = ctypes.c_int
@@ -137,6 +138,10 @@ class Oracle:
 
     def fieldsolver(self):
         self.L.orc_fieldsolver(self.h)
+
+    def set_filters(self, flags, marder_d=0.001, cerenkov_tau=0.125):
+        """Enable the Marder (bit 0) and Cherenkov (bit 1) field filters."""
+        self.L.orc_set_filters(self.h, flags, marder_d, cerenkov_tau)
 
     def countingsort(self):
         c = np.zeros(self.mx * self.my, dtype=np.int32)

@@ -28,6 +28,8 @@
 //                                1-rank ghost exchange; node averages)
 //   fieldsenergy    F:653-673
 //   countingsort    F:1303-1329
+//   divergenceclean F:867-886, suppresscerenkov F:889-907 (off by default, as
+//                   in the reference; periodic y only)
 // Additions the reference lacks (the benchmark configurations need them):
 //   conducting walls in y (particle reflection, image fold of the guard
 //   current, PEC ghost values), switchable corrections of quirks Q1-Q3.
@@ -505,8 +507,89 @@ struct Sim {
     fe[1] = 0.5 * sb * mi / (c2 * n0);
   }
 
+  // Optional field filters: Marder divergence cleaning (divergenceclean,
+  // F:867-886) and the Cherenkov filter (suppresscerenkov, F:889-907). The
+  // reference defines both and comments out their call, right after the E
+  // update (F:754-755); both read terms it stored at the end of the previous
+  // field solve, i.e. they act with E before this step's update (dive, the
+  // curls of E) and with rho from this step's push. Restated for periodic y
+  // (the reference's only boundary), in 0-based interior coordinates with
+  // both axes wrapped, without the reference's index slips (Q4 in dive, the
+  // stored rows the reference never sets).
+  int filters = 0;  // bit 0 Marder, bit 1 Cherenkov
+  double marder_d = 0.001, cer_tau = 0.125;
+  std::vector<T> fc;  // corrections: Marder ex, ey; Cherenkov ex, ey, ez (5 x mx x my)
+
+  int wxi(int i) const { return i < 0 ? i + mx : (i >= mx ? i - mx : i); }
+  int wyi(int j) const { return j < 0 ? j + my : (j >= my ? j - my : j); }
+  T e0(int c, int i, int j) { return E(c, wxi(i) + 1, wyi(j) + 1); }
+  T rho0(int i, int j) { return D(RHO, wxi(i) + 1, wyi(j) + 1); }
+  T marder_f(int i, int j) {  // dive - cva2 * rho at node (i, j)
+    const T dive = (e0(EX, i, j) - e0(EX, i - 1, j)) * idx + (e0(EY, i, j) - e0(EY, i, j - 1)) * idy;
+    return dive - cva2 * rho0(i, j);
+  }
+  T dexdy(int i, int j) { return (e0(EX, i, j + 1) - e0(EX, i, j)) * idy; }
+  T deydx(int i, int j) { return (e0(EY, i + 1, j) - e0(EY, i, j)) * idx; }
+  T dezdx(int i, int j) { return (e0(EZ, i, j) - e0(EZ, i - 1, j)) * idx; }
+  T dezdy(int i, int j) { return (e0(EZ, i, j) - e0(EZ, i, j - 1)) * idy; }
+
+  void filter_prepare() {
+    const size_t pl = (size_t)mx * my;
+    fc.assign(5 * pl, (T)0);
+    const T mdx = dt * (T)marder_d / dx, mdy = dt * (T)marder_d / dy;  // F:873-875
+    const T tau = (T)cer_tau * dt;                                     // F:895
+    const T cdx = dt * cva2 * tau / dx, cdy = dt * cva2 * tau / dy;    // F:896-897
+    for (int i = 0; i < mx; ++i)
+      for (int j = 0; j < my; ++j) {
+        const size_t k = (size_t)i * my + j;
+        if (filters & 1) {
+          const T f = marder_f(i, j);
+          fc[k] = mdx * (marder_f(i + 1, j) - f);       // F:878-881
+          fc[pl + k] = mdy * (marder_f(i, j + 1) - f);  // F:882-883
+        }
+        if (filters & 2) {
+          fc[2 * pl + k] = cdy * (deydx(i, j) - deydx(i, j - 1) - dexdy(i, j) + dexdy(i, j - 1));   // F:898-900
+          fc[3 * pl + k] = cdx * (-deydx(i, j) + deydx(i - 1, j) + dexdy(i, j) - dexdy(i - 1, j));  // F:901-903
+          fc[4 * pl + k] = cdx * (dezdx(i + 1, j) - dezdx(i, j)) + cdy * (dezdy(i, j + 1) - dezdy(i, j));  // F:904-906
+        }
+      }
+  }
+
+  void filter_apply() {  // Marder first, then the Cherenkov filter, as the commented calls
+    const size_t pl = (size_t)mx * my;
+    for (int i = 0; i < mx; ++i)
+      for (int j = 0; j < my; ++j) {
+        const size_t k = (size_t)i * my + j;
+        T& ex = E(EX, i + 1, j + 1);
+        T& ey = E(EY, i + 1, j + 1);
+        T& ez = E(EZ, i + 1, j + 1);
+        if (filters & 1) {
+          ex = ex + fc[k];
+          ey = ey + fc[pl + k];
+        }
+        if (filters & 2) {
+          ex = ex - fc[2 * pl + k];
+          ey = ey - fc[3 * pl + k];
+          ez = ez + fc[4 * pl + k];
+        }
+      }
+    // keep the periodic guards equal to the corrected interior: the x guard
+    // columns (the reference's periodic copy right after sets column 1 from
+    // column mx+1) and the ex ghost rows, which the 1-rank exchange never sets
+    for (int c : {EX, EY, EZ})
+      for (int j = 1; j <= my; ++j) {
+        E(c, 0, j) = E(c, mx, j);
+        E(c, mx + 1, j) = E(c, 1, j);
+      }
+    for (int i = 0; i <= mx + 1; ++i) {
+      E(EX, i, 0) = E(EX, i, my);
+      E(EX, i, my + 1) = E(EX, i, 1);
+    }
+  }
+
   // fieldsolver F:678-860
   void fieldsolver() {
+    if (filters) filter_prepare();
     b_half();
     periodic_x(BX);
     periodic_x(BY);
@@ -514,6 +597,7 @@ struct Sim {
     ghost_y(BY, -1, BZ, 1);
     curl_b();
     e_full();
+    if (filters) filter_apply();  // the commented calls of F:754-755
     periodic_x(EX);
     periodic_x(EY);
     periodic_x(EZ);
@@ -807,6 +891,18 @@ void orc_fieldsolver(void* h) {
   Handle* H = (Handle*)h;
   if (H->precision == 0) H->d.fieldsolver();
   else H->f.fieldsolver();
+}
+void orc_set_filters(void* h, int flags, double marder_d, double cer_tau) {
+  Handle* H = (Handle*)h;
+  if (H->precision == 0) {
+    H->d.filters = flags;
+    H->d.marder_d = marder_d;
+    H->d.cer_tau = cer_tau;
+  } else {
+    H->f.filters = flags;
+    H->f.marder_d = marder_d;
+    H->f.cer_tau = cer_tau;
+  }
 }
 void orc_countingsort(void* h, int32_t* counts_out) {
   Handle* H = (Handle*)h;

@@ -19,6 +19,7 @@ FP64_PLAIN, FP32_MIXED = 0, 1
 COMPAT_BORIS, COMPAT_FOLD, COMPAT_RHO = 1, 2, 4
 STATUS_CELL_JUMP, STATUS_NAN, STATUS_UNSORTED = 1, 2, 4
 LOAD_UNIFORM, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_WEIBEL = 0, 1, 2, 3
+FILTER_MARDER, FILTER_CERENKOV = 1, 2
 
 
 class Config(ctypes.Structure):
@@ -107,6 +108,7 @@ SIGNATURES = {
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],
     "pbpic_kernel_launches": [_PI64],
     "pbpic_counting_sort_keys_static": [_P, _I64, _I32, _P, _P, _P],
+    "pbpic_set_field_filters": [_P, _I32, ctypes.c_double, ctypes.c_double],
     "pbpic_dump": [_P, ctypes.c_char_p],
     "pbpic_restart": [_P, ctypes.c_char_p],
     "pbpic_batch_create": [ctypes.POINTER(Config), ctypes.POINTER(Loader), _I32, ctypes.POINTER(_P)],

@@ -194,6 +194,83 @@ __global__ void k_nodes(FieldParams<T> a) {
   nodes_body(a, red, blockIdx.x, gridDim.x);
 }
 
+// Optional field filters, periodic y only: Marder divergence cleaning
+// (divergenceclean, pic2d.f90:867-886) and the Cherenkov filter
+// (suppresscerenkov, pic2d.f90:889-907), whose call the reference comments
+// out right after the E update (pic2d.f90:754-755). Both act with E from
+// before the update (the reference reads terms stored by the previous field
+// solve) and with rho of this step's push: k_filter_prep computes the
+// corrections before the update, k_filter_apply adds them after it.
+template <class T>
+struct FilterParams {
+  int flags;             // bit 0 Marder, bit 1 Cherenkov
+  T mdx, mdy;            // dt * d / dx, dt * d / dy          (pic2d.f90:874-875)
+  T cdx, cdy;            // dt * cva2 * tau / dx, .. / dy       (pic2d.f90:896-897)
+  T cva2;
+  T* fc;                 // 5 planes of mx x my: Marder ex, ey; Cherenkov ex, ey, ez
+};
+
+template <class T, class Acc>
+struct FilterOps {
+  const FieldParams<T>& a;
+  __device__ T ex(int i, int j) const { return a.ex[(long long)wrapx(i, a.mx) * a.S + wrapx(j, a.my)]; }
+  __device__ T ey(int i, int j) const { return a.ey[(long long)wrapx(i, a.mx) * a.S + wrapx(j, a.my)]; }
+  __device__ T ez(int i, int j) const { return a.ez[(long long)wrapx(i, a.mx) * a.S + wrapx(j, a.my)]; }
+  __device__ T rho(int i, int j) const {
+    const long long plane = (long long)a.mx * a.S;
+    return (T)(jval<Acc>(a.jacc, 3 * plane + (long long)wrapx(i, a.mx) * a.S + wrapx(j, a.my)) * a.jscale[3]);
+  }
+  __device__ T marder_f(int i, int j, T cva2) const {  // dive - cva2 * rho at node (i, j)
+    const T dive = (ex(i, j) - ex(i - 1, j)) * a.idx + (ey(i, j) - ey(i, j - 1)) * a.idy;
+    return dive - cva2 * rho(i, j);
+  }
+  __device__ T dexdy(int i, int j) const { return (ex(i, j + 1) - ex(i, j)) * a.idy; }
+  __device__ T deydx(int i, int j) const { return (ey(i + 1, j) - ey(i, j)) * a.idx; }
+  __device__ T dezdx(int i, int j) const { return (ez(i, j) - ez(i - 1, j)) * a.idx; }
+  __device__ T dezdy(int i, int j) const { return (ez(i, j) - ez(i, j - 1)) * a.idy; }
+};
+
+template <class T, class Acc>
+__global__ void k_filter_prep(FieldParams<T> a, FilterParams<T> f) {
+  const FilterOps<T, Acc> op{a};
+  const long long pl = (long long)a.mx * a.my;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pl; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / a.my), j = (int)(k - (long long)i * a.my);
+    if (f.flags & 1) {
+      const T m = op.marder_f(i, j, f.cva2);
+      f.fc[k] = f.mdx * (op.marder_f(i + 1, j, f.cva2) - m);
+      f.fc[pl + k] = f.mdy * (op.marder_f(i, j + 1, f.cva2) - m);
+    }
+    if (f.flags & 2) {
+      f.fc[2 * pl + k] = f.cdy * (op.deydx(i, j) - op.deydx(i, j - 1) - op.dexdy(i, j) + op.dexdy(i, j - 1));
+      f.fc[3 * pl + k] = f.cdx * (-op.deydx(i, j) + op.deydx(i - 1, j) + op.dexdy(i, j) - op.dexdy(i - 1, j));
+      f.fc[4 * pl + k] = f.cdx * (op.dezdx(i + 1, j) - op.dezdx(i, j)) + f.cdy * (op.dezdy(i, j + 1) - op.dezdy(i, j));
+    }
+  }
+}
+
+template <class T>
+__global__ void k_filter_apply(FieldParams<T> a, FilterParams<T> f) {
+  const long long pl = (long long)a.mx * a.my;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pl; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / a.my), j = (int)(k - (long long)i * a.my);
+    const long long o = (long long)i * a.S + j;
+    T ex = a.ex[o], ey = a.ey[o], ez = a.ez[o];
+    if (f.flags & 1) {  // divergenceclean first, as the commented calls
+      ex = ex + f.fc[k];
+      ey = ey + f.fc[pl + k];
+    }
+    if (f.flags & 2) {
+      ex = ex - f.fc[2 * pl + k];
+      ey = ey - f.fc[3 * pl + k];
+      ez = ez + f.fc[4 * pl + k];
+    }
+    a.ex[o] = ex;
+    a.ey[o] = ey;
+    a.ez[o] = ez;
+  }
+}
+
 // Batched domains: grid row blockIdx.y works on domain blockIdx.y.
 template <class T>
 __global__ void k_bhalf_batched(const FieldParams<T>* d) {

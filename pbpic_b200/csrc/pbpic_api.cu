@@ -169,6 +169,9 @@ struct pbpic_handle {
   size_t staging_bytes = 0;
   double* rho = nullptr;
   double* dscalar = nullptr;
+  int filters = 0;               // field filters (PBPIC_FILTER_*), periodic y only
+  double marder_d = 0.001, cer_tau = 0.125;
+  void* fc = nullptr;            // filter corrections, 5 x mx x my values of the precision
   std::vector<void*> allocs;
 };
 
@@ -480,16 +483,43 @@ int do_fused_sort(pbpic_handle* h) {
 }
 
 template <class T, bool MIXED>
+FilterParams<T> filter_params(pbpic_handle* h) {
+  const pbpic_config& c = h->cfg;
+  FilterParams<T> f;
+  f.flags = h->filters;
+  const T dt = (T)c.dt, cva = (T)c.cva, cva2 = cva * cva;
+  const T d = (T)h->marder_d, tau = (T)h->cer_tau * dt;  // pic2d.f90:873, 895
+  f.mdx = dt * d / (T)c.dx;
+  f.mdy = dt * d / (T)c.dy;
+  f.cdx = dt * cva2 * tau / (T)c.dx;
+  f.cdy = dt * cva2 * tau / (T)c.dy;
+  f.cva2 = cva2;
+  f.fc = (T*)h->fc;
+  return f;
+}
+
+template <class T, bool MIXED>
 int do_fieldsolve(pbpic_handle* h) {
   cudaStream_t s = h->stream;
   FieldParams<T> a = field_params<T, MIXED>(h);
   const int rows = h->cfg.ybc == 0 ? h->cfg.my : h->cfg.my + 1;
   const int g = grid_for((int64_t)h->cfg.mx * rows, 256);
+  FilterParams<T> fp = filter_params<T, MIXED>(h);
+  const int gf = grid_for((int64_t)h->cfg.mx * h->cfg.my, 256);
+  if (h->filters) {
+    if (MIXED) k_filter_prep<T, long long><<<gf, 256, 0, s>>>(a, fp);
+    else k_filter_prep<T, double><<<gf, 256, 0, s>>>(a, fp);
+    CKLAUNCH("k_filter_prep");
+  }
   k_bhalf<T><<<g, 256, 0, s>>>(a);
   CKLAUNCH("k_bhalf");
   if (MIXED) k_efull<T, long long><<<g, 256, 0, s>>>(a);
   else k_efull<T, double><<<g, 256, 0, s>>>(a);
   CKLAUNCH("k_efull");
+  if (h->filters) {
+    k_filter_apply<T><<<gf, 256, 0, s>>>(a, fp);
+    CKLAUNCH("k_filter_apply");
+  }
   k_bhalf<T><<<g, 256, 0, s>>>(a);
   CKLAUNCH("k_bhalf");
   TRY(nodes_and_field_energy<T, MIXED>(h, h->itime + 1));
@@ -981,6 +1011,19 @@ int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every) {
     TRY(pbpic_fieldsolve(h));
     if (sort_every > 0 && h->itime % sort_every == 0) TRY(pbpic_sort(h));
   }
+  return PBPIC_OK;
+}
+
+int pbpic_set_field_filters(pbpic_handle* h, int32_t flags, double marder_d, double cerenkov_tau) {
+  TRY(check_handle(h));
+  if (flags & ~(PBPIC_FILTER_MARDER | PBPIC_FILTER_CERENKOV)) return fail(PBPIC_EINVAL, "unknown filter bits");
+  if (flags && h->cfg.ybc != PBPIC_BC_PERIODIC)
+    return fail(PBPIC_EINVAL, "the field filters are defined for periodic y only, as in the reference");
+  if (flags && !h->fc)
+    TRY(dalloc(h, &h->fc, (size_t)5 * h->cfg.mx * h->cfg.my * h->tsz));
+  h->filters = flags;
+  h->marder_d = marder_d > 0 ? marder_d : 0.001;      // pic2d.f90:873
+  h->cer_tau = cerenkov_tau > 0 ? cerenkov_tau : 0.125;  // pic2d.f90:895
   return PBPIC_OK;
 }
 
@@ -1530,6 +1573,8 @@ int batch_set_tiles(pbpic_batch* b, const int32_t* tile_rows, int groups) {
 
 int batch_step(pbpic_batch* b, int nsteps) {
   if (nsteps <= 0) return PBPIC_OK;
+  for (pbpic_handle* h : b->dom)
+    if (h->filters) return fail(PBPIC_EINVAL, "the batched form does not apply field filters");
   for (pbpic_handle* h : b->dom) {
     if (!h->sorted) TRY(do_sort<float, true>(h));
     TRY(ensure_hist(h, h->itime + nsteps + 2));

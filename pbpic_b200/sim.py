@@ -144,6 +144,10 @@ class Simulation:
     def synchronize(self):
         L.check(self._lib.pbpic_synchronize(self._h))
 
+    def set_field_filters(self, flags, marder_d=0.0, cerenkov_tau=0.0):
+        """Marder cleaning (bit 0) and the Cherenkov filter (bit 1); 0 = reference constants."""
+        L.check(self._lib.pbpic_set_field_filters(self._h, flags, marder_d, cerenkov_tau))
+
     # ---------------------------------------------------------- dump / restart
     def dump(self, directory):
         """Write the state as .npy files named like the reference's dump datasets."""

@@ -201,3 +201,53 @@ def test_energy_conservation_uniform(oracle_mod):
         tot.append(o.energies().sum())
     tot = np.array(tot)
     assert np.abs(tot / tot[0] - 1).max() < 1e-2
+
+
+def filter_corrections(cfg, yee, j4, marder_d=0.001, tau=0.125):
+    """Independent numpy statement of divergenceclean (F:867-886) and
+    suppresscerenkov (F:889-907) for periodic y: the E changes they make,
+    from E before the field solve's update and rho of the push."""
+    mx, my = cfg["mx"], cfg["my"]
+    idx, idy, dt, cva2 = 1 / cfg["dx"], 1 / cfg["dy"], cfg["dt"], cfg["cva"] ** 2
+    ex, ey, ez = (yee[c][:, :my] for c in range(3))
+    rho = j4[3][:, :my]
+    r = np.roll
+    f = (ex - r(ex, 1, 0)) * idx + (ey - r(ey, 1, 1)) * idy - cva2 * rho
+    mex = dt * marder_d / cfg["dx"] * (r(f, -1, 0) - f)
+    mey = dt * marder_d / cfg["dy"] * (r(f, -1, 1) - f)
+    cdx, cdy = dt * cva2 * tau * dt / cfg["dx"], dt * cva2 * tau * dt / cfg["dy"]
+    dexdy, deydx = (r(ex, -1, 1) - ex) * idy, (r(ey, -1, 0) - ey) * idx
+    dezdx, dezdy = (ez - r(ez, 1, 0)) * idx, (ez - r(ez, 1, 1)) * idy
+    cex = cdy * (deydx - r(deydx, 1, 1) - dexdy + r(dexdy, 1, 1))
+    cey = cdx * (-deydx + r(deydx, 1, 0) + dexdy - r(dexdy, 1, 0))
+    cez = cdx * (r(dezdx, -1, 0) - dezdx) + cdy * (r(dezdy, -1, 1) - dezdy)
+    return mex - cex, mey - cey, cez
+
+
+@pytest.mark.parametrize("flags", [1, 2, 3])
+def test_field_filters_match_numpy(oracle_mod, flags):
+    """The oracle's Marder and Cherenkov filters change E by exactly the
+    corrections an independent numpy statement computes."""
+    cfg, p, _ = fast_plasma(oracle_mod, 0, mx=16, my=12)
+    rng = np.random.default_rng(4)
+    yee = rng.normal(size=(6, 16, 13)) * 0.3
+    out = []
+    for fl in (0, flags):
+        o = oracle_mod.Oracle(**cfg)
+        o.load_particles(p)
+        o.set_fields(yee)
+        o.set_filters(fl, 0.02, 0.4)  # larger than the reference's constants, to be visible
+        e0 = o.fields()
+        o.pusher()
+        j4 = o.current()
+        o.fieldsolver()
+        out.append((e0, j4, o.fields()))
+    (e0, j4, off), (_, _, on) = out
+    want = filter_corrections(cfg, e0, j4, 0.02 if flags & 1 else 0.0, 0.4 if flags & 2 else 0.0)
+    my = cfg["my"]
+    for c in range(3):
+        got = on[c][:, :my] - off[c][:, :my]
+        assert np.abs(got - want[c]).max() <= 1e-12 * max(1.0, np.abs(want[c]).max()), (c, np.abs(got - want[c]).max(), np.abs(want[c]).max())
+        if c < 2 or flags & 2:
+            assert np.abs(want[c]).max() > 1e-6
+
