@@ -185,6 +185,19 @@ int pbpic_cell_counts(pbpic_handle* h, int32_t* counts);
 int pbpic_gauss_residual(pbpic_handle* h, double* out);
 /* Reconnected flux: half the sum of |By| along the node row my/2 times dx. */
 int pbpic_reconnected_flux(pbpic_handle* h, double* out);
+/* Energy spectra (energyspectra, pic2d.f90:1957-1990): counts[0][k-1]
+ * electrons and counts[1][k-1] ions with (gamma - 1) ms in ((k-1) de, k de],
+ * k = 1..nbins (the reference: de = 0.005 electrons, 0.005 Ti/Te ions, 1000
+ * bins). The reference's histogram indexing slip (bin, species) and its bin
+ * 0 (quirk Q6) are not reproduced: an energy of 0 counts in bin 1. */
+int pbpic_energy_spectra(pbpic_handle* h, double de_electron, double de_ion, int32_t nbins, int64_t* counts);
+/* Node values (ex ey ez bx by bz, double) along node rows rows[0..nrows)
+ * for all x and node columns cols[0..ncols) for all y, the cuts that
+ * dispersioninfo keeps for the field spectra (pic2d.f90:2124-2142):
+ * out = [nrows][mx][6] then [ncols][my][6]. Indices 0-based. */
+int pbpic_field_cuts(pbpic_handle* h, const int32_t* rows, int32_t nrows, const int32_t* cols, int32_t ncols,
+                     double* out);
+
 /* Optional field filters, off by default as in the reference, which defines
  * them and comments out their call after the E update (pic2d.f90:754-755):
  * Marder divergence cleaning (divergenceclean, pic2d.f90:867-886; marder_d

@@ -108,6 +108,8 @@ SIGNATURES = {
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],
     "pbpic_kernel_launches": [_PI64],
     "pbpic_counting_sort_keys_static": [_P, _I64, _I32, _P, _P, _P],
+    "pbpic_energy_spectra": [_P, ctypes.c_double, ctypes.c_double, _I32, _P],
+    "pbpic_field_cuts": [_P, _P, _I32, _P, _I32, _P],
     "pbpic_set_field_filters": [_P, _I32, ctypes.c_double, ctypes.c_double],
     "pbpic_dump": [_P, ctypes.c_char_p],
     "pbpic_restart": [_P, ctypes.c_char_p],

@@ -162,4 +162,61 @@ __global__ void k_flux(int mx, int my, const T* ng, double dx, double* out) {
   if (threadIdx.x == 0) *out = 0.5 * s * dx;
 }
 
+// Energy spectra (energyspectra, pic2d.f90:1957-1990): per species the
+// number of particles with (gamma - 1) ms in ((k-1) de, k de], k = 1..nbins,
+// gamma from the momenta in double. The reference's histogram is indexed
+// (bin, species) on a (species, bin) array and can take bin 0 (quirk Q6);
+// here it is counts[species][k-1] (species 0 electrons, 1 ions) and an
+// energy of exactly 0 counts in bin 1. Block histograms in shared memory.
+template <class T>
+__global__ void k_spectra(int64_t n, const uint32_t* cell, const T* ux, const T* uy, const T* uz, double mime,
+                          double de_e, double de_i, int nbins, unsigned long long* counts) {
+  extern __shared__ unsigned int hs[];  // 2 * nbins
+  for (int b = threadIdx.x; b < 2 * nbins; b += blockDim.x) hs[b] = 0u;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = ux[i], y = uy[i], z = uz[i];  // explicit rounding: no contraction
+    const double g2 = __dadd_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(x, x)), __dmul_rn(y, y)), __dmul_rn(z, z));
+    const double gama = __dsqrt_rn(g2);
+    const int sp = cw_sp(cell[i]) ? 0 : 1;  // 0 electron, 1 ion (j = 1, 2 of the reference)
+    const double ms = sp ? mime : 1.0, de = sp ? de_i : de_e;
+    const double ene = __dmul_rn(__dsub_rn(gama, 1.0), ms);
+    if (ene < __dmul_rn(de, (double)nbins)) {
+      int k = (int)ceil(__ddiv_rn(ene, de));
+      k = k < 1 ? 1 : (k > nbins ? nbins : k);
+      atomicAdd(&hs[sp * nbins + k - 1], 1u);
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < 2 * nbins; b += blockDim.x)
+    if (hs[b]) atomicAdd(&counts[b], (unsigned long long)hs[b]);
+}
+
+// Node values along chosen node rows (all x) and node columns (all y), the
+// cuts dispersioninfo stores for the field spectra (pic2d.f90:2124-2142):
+// out = [nrows][mx][6] then [ncols][my][6] (ex ey ez bx by bz), double.
+template <class T>
+__global__ void k_field_cuts(int mx, int my, const T* ng, const int32_t* rows, int nrows, const int32_t* cols,
+                             int ncols, double* out) {
+  const int64_t nr = (int64_t)nrows * mx, nt = nr + (int64_t)ncols * my;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += (int64_t)gridDim.x * blockDim.x) {
+    int i, j;
+    if (k < nr) {
+      j = rows[k / mx];
+      i = (int)(k % mx);
+    } else {
+      i = cols[(k - nr) / my];
+      j = (int)((k - nr) % my);
+    }
+    const T* g = ng + ((int64_t)i * (my + 1) + j) * 8;
+    double* o = out + k * 6;
+    o[0] = g[0];
+    o[1] = g[1];
+    o[2] = g[2];
+    o[3] = g[4];
+    o[4] = g[5];
+    o[5] = g[6];
+  }
+}
+
 }  // namespace pbd

@@ -1014,6 +1014,65 @@ int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every) {
   return PBPIC_OK;
 }
 
+int pbpic_energy_spectra(pbpic_handle* h, double de_electron, double de_ion, int32_t nbins, int64_t* counts) {
+  TRY(check_handle(h));
+  if (!counts) return fail(PBPIC_EINVAL, "null buffer");
+  if (!(de_electron > 0 && de_ion > 0) || nbins < 1 || nbins > 8192)
+    return fail(PBPIC_EINVAL, "spectra need positive bin widths and 1..8192 bins");
+  const size_t bytes = (size_t)2 * nbins * 8;
+  TRY(ensure_staging(h, bytes));
+  cudaStream_t s = h->stream;
+  CK(cudaMemsetAsync(h->staging, 0, bytes, s));
+  const int b = h->cur;
+  if (h->n > 0) {
+    const int g = grid_for(h->n, 256, 148 * 4);
+    if (h->mixed)
+      k_spectra<float><<<g, 256, (size_t)2 * nbins * 4, s>>>(h->n, h->cell[b], P<float>(h, b, 2), P<float>(h, b, 3),
+                                                            P<float>(h, b, 4), h->cfg.mime, de_electron, de_ion, nbins,
+                                                            (unsigned long long*)h->staging);
+    else
+      k_spectra<double><<<g, 256, (size_t)2 * nbins * 4, s>>>(h->n, h->cell[b], P<double>(h, b, 2),
+                                                             P<double>(h, b, 3), P<double>(h, b, 4), h->cfg.mime,
+                                                             de_electron, de_ion, nbins,
+                                                             (unsigned long long*)h->staging);
+    CKLAUNCH("k_spectra");
+  }
+  CK(cudaMemcpyAsync(counts, h->staging, bytes, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return PBPIC_OK;
+}
+
+int pbpic_field_cuts(pbpic_handle* h, const int32_t* rows, int32_t nrows, const int32_t* cols, int32_t ncols,
+                     double* out) {
+  TRY(check_handle(h));
+  const pbpic_config& c = h->cfg;
+  if (nrows < 0 || ncols < 0 || (nrows && !rows) || (ncols && !cols) || !out)
+    return fail(PBPIC_EINVAL, "null or negative cut arguments");
+  for (int k = 0; k < nrows; ++k)
+    if (rows[k] < 0 || rows[k] > c.my) return fail(PBPIC_EINVAL, "cut row outside 0..my");
+  for (int k = 0; k < ncols; ++k)
+    if (cols[k] < 0 || cols[k] > c.mx) return fail(PBPIC_EINVAL, "cut column outside 0..mx");
+  const int64_t nv = ((int64_t)nrows * c.mx + (int64_t)ncols * c.my) * 6;
+  const size_t ib = (size_t)(nrows + ncols) * 4, vb = (size_t)nv * 8;
+  TRY(ensure_staging(h, ib + vb + 16));
+  cudaStream_t s = h->stream;
+  int32_t* didx = (int32_t*)h->staging;
+  double* dval = (double*)((char*)h->staging + ((ib + 15) & ~(size_t)15));
+  if (nrows) CK(cudaMemcpyAsync(didx, rows, (size_t)nrows * 4, cudaMemcpyHostToDevice, s));
+  if (ncols) CK(cudaMemcpyAsync(didx + nrows, cols, (size_t)ncols * 4, cudaMemcpyHostToDevice, s));
+  if (nv > 0) {
+    const int g = grid_for(nv / 6, 256);
+    if (h->mixed)
+      k_field_cuts<float><<<g, 256, 0, s>>>(c.mx, c.my, (const float*)h->ng, didx, nrows, didx + nrows, ncols, dval);
+    else
+      k_field_cuts<double><<<g, 256, 0, s>>>(c.mx, c.my, (const double*)h->ng, didx, nrows, didx + nrows, ncols, dval);
+    CKLAUNCH("k_field_cuts");
+    CK(cudaMemcpyAsync(out, dval, vb, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  return PBPIC_OK;
+}
+
 int pbpic_set_field_filters(pbpic_handle* h, int32_t flags, double marder_d, double cerenkov_tau) {
   TRY(check_handle(h));
   if (flags & ~(PBPIC_FILTER_MARDER | PBPIC_FILTER_CERENKOV)) return fail(PBPIC_EINVAL, "unknown filter bits");

@@ -144,6 +144,29 @@ class Simulation:
     def synchronize(self):
         L.check(self._lib.pbpic_synchronize(self._h))
 
+    def energy_spectra(self, de_electron=0.005, de_ion=None, nbins=1000, ti_te=1.0):
+        """(2, nbins) counts, electrons then ions, of (gamma-1) ms in ((k-1) de, k de]
+        (energyspectra, pic2d.f90:1957-1990; ion bins de * Ti/Te by default)."""
+        de_ion = de_electron * ti_te if de_ion is None else de_ion
+        out = np.zeros((2, nbins), dtype=np.int64)
+        L.check(self._lib.pbpic_energy_spectra(self._h, de_electron, de_ion, nbins, L.ptr(out)))
+        return out
+
+    def field_cuts(self, rows=None, cols=None):
+        """Node values (ex ey ez bx by bz) along node rows (all x) and node columns
+        (all y), as dispersioninfo keeps them (pic2d.f90:2124-2142). Default cuts
+        are the reference's diagnostic indices (initspectdens, pic2d.f90:318-350)."""
+        if rows is None:
+            rows = [(self.my * i // 2 - self.my // 4 - 2 - 1) % self.my for i in (1, 2)]
+        if cols is None:
+            cols = [self.mx * i // 2 - self.mx // 4 - 1 for i in (1, 2)]
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        out = np.zeros(len(r) * self.mx * 6 + len(c) * self.my * 6)
+        L.check(self._lib.pbpic_field_cuts(self._h, L.ptr(r), len(r), L.ptr(c), len(c), L.ptr(out)))
+        nr = len(r) * self.mx * 6
+        return out[:nr].reshape(len(r), self.mx, 6), out[nr:].reshape(len(c), self.my, 6)
+
     def set_field_filters(self, flags, marder_d=0.0, cerenkov_tau=0.0):
         """Marder cleaning (bit 0) and the Cherenkov filter (bit 1); 0 = reference constants."""
         L.check(self._lib.pbpic_set_field_filters(self._h, flags, marder_d, cerenkov_tau))
