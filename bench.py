@@ -118,7 +118,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------- GPU
-def run_gpu(args, rank, world, dist):
+def run_gpu(args, ranks):
     import torch
 
     import pbpic_b200
@@ -126,18 +126,9 @@ def run_gpu(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
-    cfg, ld = workload(args.workload, seed_offset=rank)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    cfg, ld = workload(args.workload, seed_offset=ranks.replica_seed(0))
+    barrier, max_over_ranks = ranks.barrier, ranks.max
+    world = ranks.world
 
     results = {}
     sampler = ClockSampler(dev)
@@ -332,25 +323,19 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as tdist
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = tdist
-    cfg, res, clocks, e2e, ens = run_gpu(args, rank, world, dist)
+    from pbpic_b200.replicas import Ranks
+    ranks = Ranks("nccl")
+    cfg, res, clocks, e2e, ens = run_gpu(args, ranks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_sample(args.workload, 4)
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return
     m = res["fp32"]
     n = m["n"]
     K = args.steps
-    value = world * n * K / (m["total_ms"] * 1e-3)
+    value = ranks.throughput(n, K, m["total_ms"])
     peak, peak_kind = measured_peak_hbm()
     bytes_push = 48.0 * n  # read + write of cell (4 B), offsets (2x4 B), momenta (3x4 B)
     achieved_push = bytes_push / (m["t_push"] * 1e-3) / 1e9
