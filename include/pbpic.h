@@ -253,6 +253,34 @@ int pbpic_dump(pbpic_handle* h, const char* dir);
  * bit). */
 int pbpic_restart(pbpic_handle* h, const char* dir);
 
+/* ----------------------------------------------------------------- y slabs */
+/* Device-side pieces of the y-slab decomposition, the reference's 1-D domain
+ * decomposition along y over MPI ranks (pic2d.f90:206-212; its ghost-row and
+ * particle exchanges, pic2d.f90:701-835, 1072-1146). Each rank steps an
+ * extended domain (its own rows plus ghost bands of neighbouring rows) and
+ * exchanges, after each step, the ghost field rows and the particles of the
+ * bands next to its neighbours (pbpic_b200/slab.py drives it). Bands travel
+ * as reference particle records of the global grid (pbpic_particle_f32 for
+ * the mixed form, _f64 for the plain form) in DEVICE memory: grid =
+ * my_global * ix + (local row + row_offset) + 1. */
+/* Copies the particles in local rows [y_lo, y_hi) to dst_dev (at most cap
+ * records); *n = their number (ECAPACITY when above cap). Order kept. */
+int pbpic_band_extract(pbpic_handle* h, int32_t y_lo, int32_t y_hi, int32_t my_global, int32_t row_offset,
+                       void* dst_dev, int64_t cap, int64_t* n);
+/* Keeps only the particles in local rows [y_lo, y_hi), in their order. */
+int pbpic_band_keep(pbpic_handle* h, int32_t y_lo, int32_t y_hi);
+/* Appends n records from device memory; local row = global row - row_offset. */
+int pbpic_band_append(pbpic_handle* h, const void* src_dev, int64_t n, int32_t my_global, int32_t row_offset);
+/* Rows j0 .. j0+nrows-1 of the six field planes to / from device memory as
+ * [6][mx][nrows] values of the handle's precision; setting them recomputes
+ * the node averages. */
+int pbpic_field_rows_get(pbpic_handle* h, int32_t j0, int32_t nrows, void* dst_dev);
+int pbpic_field_rows_set(pbpic_handle* h, int32_t j0, int32_t nrows, const void* src_dev);
+/* Energies (electron KE, ion KE, E, B) of the particles in rows [y_lo,
+ * y_hi) and of the node rows [y_lo, y_hi); node rows wall_lo and wall_hi
+ * (global walls; -1: none) weigh 1/2 as in the conducting-wall sums. */
+int pbpic_energies_rows(pbpic_handle* h, int32_t y_lo, int32_t y_hi, int32_t wall_lo, int32_t wall_hi, double* out);
+
 /* ------------------------------------------------------------ batched form */
 /* Many independent domains of uneven grid size and particle count advanced
  * together. Every phase of a step runs once for all domains: persistent

@@ -112,6 +112,12 @@ SIGNATURES = {
     "pbpic_field_cuts": [_P, _P, _I32, _P, _I32, _P],
     "pbpic_set_field_filters": [_P, _I32, ctypes.c_double, ctypes.c_double],
     "pbpic_dump": [_P, ctypes.c_char_p],
+    "pbpic_band_extract": [_P, _I32, _I32, _I32, _I32, _P, _I64, _PI64],
+    "pbpic_band_keep": [_P, _I32, _I32],
+    "pbpic_band_append": [_P, _P, _I64, _I32, _I32],
+    "pbpic_field_rows_get": [_P, _I32, _I32, _P],
+    "pbpic_field_rows_set": [_P, _I32, _I32, _P],
+    "pbpic_energies_rows": [_P, _I32, _I32, _I32, _I32, _P],
     "pbpic_restart": [_P, ctypes.c_char_p],
     "pbpic_batch_create": [ctypes.POINTER(Config), ctypes.POINTER(Loader), _I32, ctypes.POINTER(_P)],
     "pbpic_batch_destroy": [_P],

@@ -1,0 +1,175 @@
+// Kernels of the y-slab decomposition (one rank per slab of cell rows, the
+// reference's 1-D domain decomposition along y, pic2d.f90:206-212). Each rank
+// steps an extended domain: its own rows plus ghost bands of rows copied
+// from the neighbouring slabs. These kernels move particles and field rows in
+// and out of such a domain and sum energies over its own rows:
+//   k_band_flags / k_band_out    particles of a band of rows -> reference
+//                                records, rows renumbered to the global grid
+//   k_band_keep                  stable compaction to a band of rows
+//   k_band_in                    reference records (global grid) -> appended
+//   k_rows_get / k_rows_set      rows of the six field planes
+//   k_kinetic_rows, k_field_energy_rows   energy sums over the own rows
+#pragma once
+#include "device_common.cuh"
+#include "kernels_misc.cuh"
+
+namespace pbd {
+
+static __global__ void k_band_flags(int64_t n, const uint32_t* cell, int y_lo, int y_hi, int32_t* flags) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == n) {
+      flags[i] = 0;
+      continue;
+    }
+    const int iy = cw_iy(cell[i]);
+    flags[i] = (iy >= y_lo && iy < y_hi) ? 1 : 0;
+  }
+}
+
+// Particles with a flag to out[pos[i]] as reference records of the global
+// grid: grid = my_global * ix + (iy + row_offset) + 1, q = +1 ion / -1 electron.
+template <class T, class R>
+__global__ void k_band_out(int64_t n, const uint32_t* cell, const T* dx, const T* dy, const T* ux, const T* uy,
+                           const T* uz, const int32_t* pid, const int32_t* pos, int my_global, int row_offset,
+                           RefRec<R>* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (pos[i + 1] == pos[i]) continue;  // not in the band
+    const uint32_t w = cell[i];
+    RefRec<R> r;
+    r.dx = (R)dx[i];
+    r.dy = (R)dy[i];
+    r.ux = (R)ux[i];
+    r.uy = (R)uy[i];
+    r.uz = (R)uz[i];
+    r.grid = my_global * cw_ix(w) + cw_iy(w) + row_offset + 1;
+    r.q = cw_sp(w) ? -1 : 1;
+    r.pid = pid ? pid[i] : 0;
+    out[pos[i]] = r;
+  }
+}
+
+// Stable compaction of the flagged particles into the other buffer.
+template <class T>
+__global__ void k_band_keep(int64_t n, const int32_t* pos, const uint32_t* ci, const T* dxi, const T* dyi,
+                            const T* uxi, const T* uyi, const T* uzi, const int32_t* pidi, uint32_t* co, T* dxo,
+                            T* dyo, T* uxo, T* uyo, T* uzo, int32_t* pido) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (pos[i + 1] == pos[i]) continue;
+    const int64_t d = pos[i];
+    co[d] = ci[i];
+    dxo[d] = dxi[i];
+    dyo[d] = dyi[i];
+    uxo[d] = uxi[i];
+    uyo[d] = uyi[i];
+    uzo[d] = uzi[i];
+    if (pido) pido[d] = pidi[i];
+  }
+}
+
+// Reference records of the global grid appended at base: local row =
+// global row - row_offset, which must fall in [0, my) (status bit 8 and the
+// record is written as an empty electron at cell (0, 0) with zero momentum
+// otherwise, so that the count stays consistent).
+template <class T, class R>
+__global__ void k_band_in(const RefRec<R>* in, int64_t n, int my_global, int row_offset, int mx, int my, int64_t base,
+                          uint32_t* cell, T* dx, T* dy, T* ux, T* uy, T* uz, int32_t* pid, int* status) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const RefRec<R> r = in[i];
+    const int g = r.grid - 1;
+    const int ix = g / my_global, gy = g - ix * my_global;
+    const int iy = gy - row_offset;
+    const bool ok = g >= 0 && ix < mx && iy >= 0 && iy < my && (r.q == 1 || r.q == -1);
+    const int64_t d = base + i;
+    if (!ok) atomicOr(status, 8);
+    cell[d] = ok ? cw_make(ix, iy, r.q < 0 ? 1 : 0) : cw_make(0, 0, 1);
+    dx[d] = ok ? (T)r.dx : T(0);
+    dy[d] = ok ? (T)r.dy : T(0);
+    ux[d] = ok ? (T)r.ux : T(0);
+    uy[d] = ok ? (T)r.uy : T(0);
+    uz[d] = ok ? (T)r.uz : T(0);
+    if (pid) pid[d] = r.pid;
+  }
+}
+
+// Rows j0 .. j0+nrows-1 of the six planes <-> buf[(c * mx + i) * nrows + r].
+template <class T>
+struct Planes6 {
+  T* f[6];
+};
+
+template <class T>
+__global__ void k_rows_get(Planes6<T> p, int mx, int S, int j0, int nrows, T* buf) {
+  const int64_t tot = (int64_t)6 * mx * nrows;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(k / ((int64_t)mx * nrows));
+    const int64_t rem = k - (int64_t)c * mx * nrows;
+    const int i = (int)(rem / nrows), r = (int)(rem - (int64_t)i * nrows);
+    buf[k] = p.f[c][(int64_t)i * S + j0 + r];
+  }
+}
+
+template <class T>
+__global__ void k_rows_set(Planes6<T> p, int mx, int S, int j0, int nrows, const T* buf) {
+  const int64_t tot = (int64_t)6 * mx * nrows;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(k / ((int64_t)mx * nrows));
+    const int64_t rem = k - (int64_t)c * mx * nrows;
+    const int i = (int)(rem / nrows), r = (int)(rem - (int64_t)i * nrows);
+    p.f[c][(int64_t)i * S + j0 + r] = buf[k];
+  }
+}
+
+// Kinetic energy of the particles in rows [y_lo, y_hi), as k_kinetic.
+template <class T, bool MIXED>
+__global__ void k_kinetic_rows(int64_t n, const uint32_t* cell, const T* ux, const T* uy, const T* uz, T ms_i,
+                               int y_lo, int y_hi, double* part) {
+  __shared__ double red[32];
+  double ke[2] = {0, 0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = cell[i];
+    const int iy = cw_iy(w);
+    if (iy < y_lo || iy >= y_hi) continue;
+    using A = M<T, MIXED>;
+    const T a = ux[i], b = uy[i], c = uz[i];
+    const T usq = A::mad(c, c, A::mad(b, b, A::mul(a, a)));
+    const T g = A::sqrt(A::mad(c, c, A::mad(b, b, A::mad(a, a, T(1)))));
+    const int sp = cw_sp(w);
+    const T ms = sp ? T(1) : ms_i;
+    const double e = MIXED ? (double)A::mul(A::div(usq, A::add(g, T(1))), ms) : (double)A::mul(A::sub(g, T(1)), ms);
+    ke[sp ? 0 : 1] += e;
+  }
+  const double s0 = block_sum(ke[0], red), s1 = block_sum(ke[1], red);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s0;
+    part[2 * blockIdx.x + 1] = s1;
+  }
+}
+
+// Field energy sums over node rows [y_lo, y_hi) of the node grid (the
+// fieldsenergy sums of k_nodes); node rows equal to wall_lo or wall_hi
+// (global walls) weigh 1/2.
+template <class T>
+__global__ void k_field_energy_rows(int mx, int my, const T* ng, int y_lo, int y_hi, int wall_lo, int wall_hi,
+                                    double* part) {
+  __shared__ double red[32];
+  const int rows = y_hi - y_lo;
+  const int64_t nn = (int64_t)mx * rows;
+  double se = 0.0, sb = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k / rows), j = y_lo + (int)(k - (int64_t)(k / rows) * rows);
+    const T* g = ng + ((int64_t)i * (my + 1) + j) * 8;
+    const T e2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    const T b2 = g[4] * g[4] + g[5] * g[5] + g[6] * g[6];
+    const double w = (j == wall_lo || j == wall_hi) ? 0.5 : 1.0;
+    se += w * (double)e2;
+    sb += w * (double)b2;
+  }
+  se = block_sum(se, red);
+  sb = block_sum(sb, red);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = se;
+    part[2 * blockIdx.x + 1] = sb;
+  }
+}
+
+}  // namespace pbd

@@ -20,6 +20,7 @@
 #include "kernels_field.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_push.cuh"
+#include "kernels_slab.cuh"
 #include "kernels_sort.cuh"
 #include "npy_io.h"
 #include "pic_common.h"
@@ -172,6 +173,8 @@ struct pbpic_handle {
   int filters = 0;               // field filters (PBPIC_FILTER_*), periodic y only
   double marder_d = 0.001, cer_tau = 0.125;
   void* fc = nullptr;            // filter corrections, 5 x mx x my values of the precision
+  int32_t* band_flags = nullptr;    // slab exchange: flags / positions (capacity + 2)
+  int32_t* band_scratch = nullptr;  // and their scan's chunk totals
   std::vector<void*> allocs;
 };
 
@@ -839,7 +842,7 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
   const int64_t sc = std::max(scan_scratch_ints(radix_hist_ints((int64_t)capn)), scan_scratch_ints(h->ncells + 1));
   A(&h->scan_scratch, (size_t)sc * 4);
   A(&h->rho, (size_t)pe * 8);
-  A(&h->dscalar, 16);
+  A(&h->dscalar, 64);  // scalars of the diagnostics (up to 4 doubles)
   if (r != PBPIC_OK) {
     pbpic_destroy(h);
     return r;
@@ -2006,6 +2009,173 @@ int pbpic_restart(pbpic_handle* h, const char* dir) {
   TRY(check_handle(h));
   if (!dir) return fail(PBPIC_EINVAL, "null directory");
   return DISPATCH(h, do_restart, h, std::string(dir));
+}
+
+}  // extern "C"
+
+// ================================================================ y slabs
+// Device-side pieces of the y-slab decomposition (kernels_slab.cuh); the
+// driver that exchanges ghost bands between ranks is pbpic_b200/slab.py.
+namespace {
+
+int band_buffers(pbpic_handle* h) {
+  if (h->band_flags) return PBPIC_OK;
+  const int64_t m = std::max<int64_t>(h->cap, 1) + 2;
+  TRY(dalloc(h, &h->band_flags, (size_t)m * 4));
+  TRY(dalloc(h, &h->band_scratch, (size_t)scan_scratch_ints(m) * 4));
+  return PBPIC_OK;
+}
+
+// Positions of the particles in rows [y_lo, y_hi): exclusive scan of the
+// flags in h->band_flags; returns their number.
+int band_positions(pbpic_handle* h, int y_lo, int y_hi, int64_t* count) {
+  TRY(band_buffers(h));
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  k_band_flags<<<grid_for(n + 1, 256), 256, 0, s>>>(n, h->cell[h->cur], y_lo, y_hi, h->band_flags);
+  CKLAUNCH("k_band_flags");
+  TRY(scan_excl(s, h->band_flags, n + 1, h->band_scratch));
+  int32_t c = 0;
+  CK(cudaMemcpyAsync(&c, h->band_flags + n, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *count = c;
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_band_extract(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_offset, void* dst, int64_t cap,
+                    int64_t* nout) {
+  int64_t c = 0;
+  TRY(band_positions(h, y_lo, y_hi, &c));
+  if (nout) *nout = c;
+  if (c > cap) return fail(PBPIC_ECAPACITY, "the band holds more particles than the destination");
+  const int b = h->cur;
+  if (h->n > 0 && c > 0) {
+    k_band_out<T, T><<<grid_for(h->n, 256), 256, 0, h->stream>>>(h->n, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
+                                                                 P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4),
+                                                                 h->pid[b], h->band_flags, my_global, row_offset,
+                                                                 (RefRec<T>*)dst);
+    CKLAUNCH("k_band_out");
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_band_keep(pbpic_handle* h, int y_lo, int y_hi) {
+  int64_t c = 0;
+  TRY(band_positions(h, y_lo, y_hi, &c));
+  const int b = h->cur, o = 1 - b;
+  if (h->n > 0) {
+    k_band_keep<T><<<grid_for(h->n, 256), 256, 0, h->stream>>>(
+        h->n, h->band_flags, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4),
+        h->pid[b], h->cell[o], P<T>(h, o, 0), P<T>(h, o, 1), P<T>(h, o, 2), P<T>(h, o, 3), P<T>(h, o, 4), h->pid[o]);
+    CKLAUNCH("k_band_keep");
+    h->cur = o;
+  }
+  h->n = c;
+  return set_unsorted_tiles(h);
+}
+
+template <class T, bool MIXED>
+int do_band_append(pbpic_handle* h, const void* src, int64_t n, int my_global, int row_offset) {
+  if (n < 0) return fail(PBPIC_EINVAL, "negative count");
+  if (h->n + n > h->cap) return fail(PBPIC_ECAPACITY, "appending the band exceeds the capacity");
+  if (n == 0) return PBPIC_OK;
+  if (!src) return fail(PBPIC_EINVAL, "null band");
+  cudaStream_t s = h->stream;
+  const int b = h->cur;
+  CK(cudaMemsetAsync(h->dscalar, 0, 4, s));
+  k_band_in<T, T><<<grid_for(n, 256), 256, 0, s>>>((const RefRec<T>*)src, n, my_global, row_offset, h->cfg.mx,
+                                                   h->cfg.my, h->n, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
+                                                   P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b],
+                                                   (int*)h->dscalar);
+  CKLAUNCH("k_band_in");
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, h->dscalar, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  h->n += n;
+  TRY(set_unsorted_tiles(h));
+  if (st & 8) return fail(PBPIC_EINVAL, "band record outside this domain's rows or with q not +-1");
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_field_rows(pbpic_handle* h, int j0, int nrows, void* buf, bool set) {
+  if (j0 < 0 || nrows < 0 || j0 + nrows > h->S) return fail(PBPIC_EINVAL, "field rows outside 0..my");
+  if (nrows == 0) return PBPIC_OK;
+  if (!buf) return fail(PBPIC_EINVAL, "null buffer");
+  Planes6<T> p;
+  for (int c = 0; c < 6; ++c) p.f[c] = (T*)h->f[c];
+  const int g = grid_for((int64_t)6 * h->cfg.mx * nrows, 256);
+  if (set) {
+    k_rows_set<T><<<g, 256, 0, h->stream>>>(p, h->cfg.mx, h->S, j0, nrows, (const T*)buf);
+    CKLAUNCH("k_rows_set");
+    TRY((nodes_and_field_energy<T, MIXED>(h, h->itime)));
+  } else {
+    k_rows_get<T><<<g, 256, 0, h->stream>>>(p, h->cfg.mx, h->S, j0, nrows, (T*)buf);
+    CKLAUNCH("k_rows_get");
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return PBPIC_OK;
+}
+
+template <class T, bool MIXED>
+int do_energies_rows(pbpic_handle* h, int y_lo, int y_hi, int wall_lo, int wall_hi, double* out) {
+  const pbpic_config& c = h->cfg;
+  if (y_lo < 0 || y_hi > h->S || y_lo > y_hi) return fail(PBPIC_EINVAL, "rows outside 0..my");
+  cudaStream_t s = h->stream;
+  const int b = h->cur;
+  k_kinetic_rows<T, MIXED><<<h->nke, 256, 0, s>>>(h->n, h->cell[b], P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4),
+                                                   (T)c.mime, y_lo, std::min(y_hi, c.my), h->ke_part);
+  CKLAUNCH("k_kinetic_rows");
+  k_field_energy_rows<T><<<h->nfe, 256, 0, s>>>(c.mx, c.my, (const T*)h->ng, y_lo, y_hi, wall_lo, wall_hi,
+                                               h->fe_part);
+  CKLAUNCH("k_field_energy_rows");
+  k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->nke, h->fe_part, h->nfe, fe_scale(c), fb_scale(c), h->dscalar);
+  CKLAUNCH("k_energy_row");
+  CK(cudaMemcpyAsync(out, h->dscalar, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return PBPIC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbpic_band_extract(pbpic_handle* h, int32_t y_lo, int32_t y_hi, int32_t my_global, int32_t row_offset,
+                       void* dst_dev, int64_t cap, int64_t* n) {
+  TRY(check_handle(h));
+  if (y_lo < 0 || y_hi > h->cfg.my || y_lo > y_hi || my_global < 1) return fail(PBPIC_EINVAL, "bad band rows");
+  return DISPATCH(h, do_band_extract, h, y_lo, y_hi, my_global, row_offset, dst_dev, cap, n);
+}
+
+int pbpic_band_keep(pbpic_handle* h, int32_t y_lo, int32_t y_hi) {
+  TRY(check_handle(h));
+  if (y_lo < 0 || y_hi > h->cfg.my || y_lo > y_hi) return fail(PBPIC_EINVAL, "bad band rows");
+  return DISPATCH(h, do_band_keep, h, y_lo, y_hi);
+}
+
+int pbpic_band_append(pbpic_handle* h, const void* src_dev, int64_t n, int32_t my_global, int32_t row_offset) {
+  TRY(check_handle(h));
+  if (my_global < 1) return fail(PBPIC_EINVAL, "bad global row count");
+  return DISPATCH(h, do_band_append, h, src_dev, n, my_global, row_offset);
+}
+
+int pbpic_field_rows_get(pbpic_handle* h, int32_t j0, int32_t nrows, void* dst_dev) {
+  TRY(check_handle(h));
+  return DISPATCH(h, do_field_rows, h, j0, nrows, dst_dev, false);
+}
+
+int pbpic_field_rows_set(pbpic_handle* h, int32_t j0, int32_t nrows, const void* src_dev) {
+  TRY(check_handle(h));
+  return DISPATCH(h, do_field_rows, h, j0, nrows, const_cast<void*>(src_dev), true);
+}
+
+int pbpic_energies_rows(pbpic_handle* h, int32_t y_lo, int32_t y_hi, int32_t wall_lo, int32_t wall_hi, double* out) {
+  TRY(check_handle(h));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  return DISPATCH(h, do_energies_rows, h, y_lo, y_hi, wall_lo, wall_hi, out);
 }
 
 }  // extern "C"

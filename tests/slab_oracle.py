@@ -1,0 +1,80 @@
+"""A slab engine over the CPU oracle (test infrastructure): the same
+interface as pbpic_b200.slab.GpuEngine, with host arrays, so the slab driver
+and its torch.distributed transport can run as gloo ranks without a GPU."""
+import numpy as np
+import torch
+
+from pbpic_b200 import _lib as L
+
+
+class OracleEngine:
+    def __init__(self, O, cfg, lay):
+        self.O = O
+        self.lay = lay
+        self.cfg = dict(cfg, my=lay.my_local)
+        self.o = O.Oracle(**self.cfg)
+        self.mx = cfg["mx"]
+
+    def load(self, p, f):
+        self.o.load_particles(p, capacity=4 * len(p) + 64)
+        self.o.set_fields(f)
+
+    def _rows(self, p):
+        g = p["grid"].astype(np.int64) - 1
+        return g // self.lay.my_local, g % self.lay.my_local
+
+    def extract(self, y_lo, y_hi):
+        p = self.o.particles()
+        ix, iy = self._rows(p)
+        m = (iy >= y_lo) & (iy < y_hi)
+        q = p[m].copy()
+        q["grid"] = (ix[m] * self.lay.my + iy[m] + self.lay.row_offset + 1).astype(np.int32)
+        return torch.from_numpy(q.view(np.uint8).copy())
+
+    def keep(self, y_lo, y_hi):
+        p = self.o.particles()
+        _, iy = self._rows(p)
+        self.o.load_particles(p[(iy >= y_lo) & (iy < y_hi)], capacity=4 * len(p) + 64)
+
+    def append(self, band, row_offset):
+        q = band.numpy().view(self.O.PARTICLE).copy()
+        if len(q) == 0:
+            return
+        g = q["grid"].astype(np.int64) - 1
+        ix, gy = g // self.lay.my, g % self.lay.my
+        iy = gy - row_offset
+        assert ((iy >= 0) & (iy < self.lay.my_local)).all()
+        q["grid"] = (ix * self.lay.my_local + iy + 1).astype(np.int32)
+        p = np.concatenate([self.o.particles(), q])
+        self.o.load_particles(p, capacity=4 * len(p) + 64)
+
+    def field_rows(self, j0, nrows):
+        f = self.o.fields()[:, :, j0:j0 + nrows]
+        return torch.from_numpy(np.ascontiguousarray(f).reshape(-1).copy())
+
+    def set_field_rows(self, j0, nrows, buf):
+        f = self.o.fields()
+        f[:, :, j0:j0 + nrows] = buf.numpy().reshape(6, self.mx, nrows)
+        self.o.set_fields(f)
+
+    def push(self):
+        self.o.pusher()
+
+    def fieldsolve(self):
+        self.o.fieldsolver()
+
+    def sort(self):
+        self.o.countingsort()
+
+    def own_particles(self):
+        p = self.o.particles()
+        ix, iy = self._rows(p)
+        m = (iy >= self.lay.lo) & (iy < self.lay.hi)
+        q = p[m].copy()
+        q["grid"] = (ix[m] * self.lay.my + iy[m] - self.lay.gl + self.lay.y0 + 1).astype(np.int32)
+        return q
+
+    def own_fields(self):
+        f = self.o.fields()
+        out = f[:, :, self.lay.lo:self.lay.hi]
+        return out, (f[:, :, self.lay.my_local] if self.lay.wall_hi >= 0 else None)

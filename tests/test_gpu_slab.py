@@ -1,0 +1,100 @@
+"""The y-slab decomposition against the single-domain run of the same
+plasma: W slabs (W = 1, 2, 3, stepped in one process on one GPU, exchanging
+their ghost bands between steps) reproduce the single domain's particles
+(matched by id), fields and energies. FP64 plain: within 1e-12 relative (the
+order of the FP64 current sums differs); FP32 mixed: within FP32 rounding."""
+import numpy as np
+import pytest
+
+from pbpic_b200 import _lib as L
+from pbpic_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def global_case(kind):
+    if kind == "uniform":
+        cfg, ld = configs.uniform_c1(seed=21, mx=24, my=30, ppc=4)
+        ld = dict(ld, vthe=0.3, vthi=0.1)
+        return cfg, ld
+    return configs.harris(24, 30, 4, seed=22)
+
+
+def run_single(cfg, ld, precision, steps):
+    from pbpic_b200.sim import Simulation
+    n = 2 * ld["ppc"] * cfg["mx"] * cfg["my"]
+    s = Simulation(**cfg, precision=precision, capacity=n, track_pid=True)
+    s.init_plasma(**ld)
+    p0, f0 = s.particles(), s.fields()
+    for _ in range(steps):
+        s.pusher()
+        s.fieldsolver()
+        s.countingsort()
+    return s, p0, f0
+
+
+def run_slabs(cfg, p0, f0, precision, world, steps):
+    from pbpic_b200.slab import GpuEngine, InProcess, Layout, SlabRun, scatter_plasma
+    slabs = {}
+    for r in range(world):
+        lay = Layout(cfg["my"], world, r, cfg["ybc"])
+        e = GpuEngine(cfg, lay, precision, capacity=2 * len(p0), track_pid=True)  # own rows + ghost bands
+        p, f = scatter_plasma(p0, f0, lay)
+        e.sim.load_particles(p)
+        e.sim.load_fields(f)
+        slabs[r] = e
+    run = SlabRun(slabs, InProcess())
+    run.start()
+    run.step(steps)
+    return slabs
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+@pytest.mark.parametrize("kind", ["uniform", "harris"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_slabs_match_single_domain(gpu_lib, kind, world, precision):
+    cfg, ld = global_case(kind)
+    steps = 5
+    single, p0, f0 = run_single(cfg, ld, precision, steps)
+    slabs = run_slabs(cfg, p0, f0, precision, world, steps)
+    ps = single.particles()
+    n_own = 0
+    for e in slabs.values():
+        g = e.sim.particles()["grid"].astype(np.int64) - 1
+        iy = g % e.lay.my_local
+        n_own += int(((iy >= e.lay.lo) & (iy < e.lay.hi)).sum())
+    assert n_own == len(ps)  # every particle in exactly one slab's own rows
+    own = []
+    for e in slabs.values():
+        p = e.sim.particles()
+        g = p["grid"].astype(np.int64) - 1
+        ix, iy = g // e.lay.my_local, g % e.lay.my_local
+        m = (iy >= e.lay.lo) & (iy < e.lay.hi)
+        q = p[m].copy()
+        q["grid"] = (ix[m] * cfg["my"] + iy[m] - e.lay.gl + e.lay.y0 + 1).astype(np.int32)
+        own.append(q)
+    pg = np.concatenate(own)
+    pg, ps = pg[np.argsort(pg["pid"])], ps[np.argsort(ps["pid"])]
+    assert np.array_equal(pg["pid"], ps["pid"])
+    tol = 1e-12 if precision == "fp64" else 2e-5
+    bad = pg["grid"] != ps["grid"]
+    assert bad.sum() <= (0 if precision == "fp64" else 2)
+    for c in ("dx", "dy", "ux", "uy", "uz"):
+        d = np.abs(pg[c][~bad] - ps[c][~bad]).max()
+        assert d <= tol * max(1.0, np.abs(ps[c]).max()), (c, d)
+    fs = single.fields()
+    fg = np.zeros_like(fs)
+    my = cfg["my"]
+    for e in slabs.values():
+        lay = e.lay
+        fl = e.sim.fields()
+        fg[:, :, lay.y0:lay.y1] = fl[:, :, lay.lo:lay.hi]
+        if lay.wall_hi >= 0:
+            fg[:, :, my] = fl[:, :, lay.my_local]
+    rows = my + 1 if cfg["ybc"] == L.BC_CONDUCTING else my
+    ftol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.abs(fg[:, :, :rows] - fs[:, :, :rows]).max() <= ftol * np.abs(fs).max()
+    es = single.energies()
+    eg = sum(e.energies() for e in slabs.values())
+    etol = 1e-11 if precision == "fp64" else 1e-5
+    assert np.allclose(eg, es, rtol=etol, atol=etol * np.abs(es).max())
