@@ -134,7 +134,10 @@ def run_gpu(args, ranks):
     sampler = ClockSampler(dev)
     for prec in (["fp32"] if args.no_fp64 else ["fp32", "fp64"]):
         n = pbpic_b200.Simulation(**cfg, precision=prec, capacity=1).loader_count(**ld)
-        with pbpic_b200.Simulation(**cfg, precision=prec, capacity=n) as s:
+        # sort every step: the push and the counting sort are timed as separate
+        # calls; another cadence: the library's default, the push sorts anyway
+        opts = pbpic_b200.OPT_NO_AUTOSORT if args.sort_every == 1 else 0
+        with pbpic_b200.Simulation(**cfg, precision=prec, capacity=n, options=opts) as s:
             s.set_stream(stream.cuda_stream)
             s.init_plasma(**ld)
             s.step(args.warmup, sort_every=args.sort_every)

@@ -20,6 +20,7 @@ COMPAT_BORIS, COMPAT_FOLD, COMPAT_RHO = 1, 2, 4
 STATUS_CELL_JUMP, STATUS_NAN, STATUS_UNSORTED = 1, 2, 4
 LOAD_UNIFORM, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_WEIBEL = 0, 1, 2, 3
 FILTER_MARDER, FILTER_CERENKOV = 1, 2
+OPT_NO_AUTOSORT = 1
 
 
 class Config(ctypes.Structure):
@@ -29,7 +30,7 @@ class Config(ctypes.Structure):
         ("cva", ctypes.c_double), ("mime", ctypes.c_double), ("in0", ctypes.c_double),
         ("ybc", ctypes.c_int32), ("precision", ctypes.c_int32), ("compat", ctypes.c_int32),
         ("track_pid", ctypes.c_int32), ("capacity", ctypes.c_int64),
-        ("tile_rows", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("tile_rows", ctypes.c_int32), ("options", ctypes.c_int32),
     ]
 
 

@@ -363,6 +363,7 @@ int do_fused_sort(pbpic_handle* h);
 template <class T, bool MIXED>
 int do_sort(pbpic_handle* h) {
   if (h->hist_valid) return do_fused_sort<T, MIXED>(h);
+  if (h->sorted) return PBPIC_OK;  // already in cell order (tables current)
   cudaStream_t s = h->stream;
   const int64_t n = h->n;
   CK(cudaMemsetAsync(h->counts, 0, (size_t)(h->ncells + 1) * 4, s));
@@ -394,6 +395,8 @@ int do_sort(pbpic_handle* h) {
 
 template <class T, bool MIXED>
 int do_push(pbpic_handle* h) {
+  const bool autosort = !(h->cfg.options & PBPIC_OPT_NO_AUTOSORT) && h->fused_ok;
+  if (autosort && !h->sorted) TRY((do_sort<T, MIXED>(h)));
   cudaStream_t s = h->stream;
   TRY(ensure_hist(h, h->itime + 2));
   CK(cudaMemsetAsync(h->jacc, 0, (size_t)4 * plane_elems(h) * 8, s));
@@ -407,6 +410,7 @@ int do_push(pbpic_handle* h) {
   CKLAUNCH("k_energy_row");
   h->hist_valid = hist;
   h->sorted = false;
+  if (autosort) TRY((do_fused_sort<T, MIXED>(h)));
   return PBPIC_OK;
 }
 
@@ -784,6 +788,7 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
     return fail(PBPIC_EINVAL, "unknown precision");
   if (c.capacity < 0 || c.capacity > 0x7fffff00ll) return fail(PBPIC_EINVAL, "capacity must be in [0, 2^31)");
   if (c.compat & ~7) return fail(PBPIC_EINVAL, "unknown compat bits");
+  if (c.options & ~PBPIC_OPT_NO_AUTOSORT) return fail(PBPIC_EINVAL, "unknown option bits");
   const double cfl = c.cva * c.dt * sqrt(1.0 / (c.dx * c.dx) + 1.0 / (c.dy * c.dy));
   if (!(cfl < 1.0)) return fail(PBPIC_EINVAL, "time step violates the CFL condition c*dt*sqrt(1/dx^2+1/dy^2) < 1");
   if (c.cva * c.dt / std::min(c.dx, c.dy) >= 1.0)

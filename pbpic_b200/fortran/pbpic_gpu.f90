@@ -31,7 +31,7 @@ module pbpic_gpu
         real(c_double) :: dx, dy, dt, cva, mime, in0
         integer(c_int32_t) :: ybc, precision, compat, track_pid
         integer(c_int64_t) :: capacity
-        integer(c_int32_t) :: tile_rows, reserved
+        integer(c_int32_t) :: tile_rows, options
     end type
 
     type, bind(c) :: c_particle

@@ -14,12 +14,12 @@ from . import _lib as L
 
 class Simulation:
     def __init__(self, mx, my, dx, dy, dt, cva, mime, in0, ybc=L.BC_PERIODIC, precision="fp64",
-                 compat=0, track_pid=False, capacity=0, tile_rows=0):
+                 compat=0, track_pid=False, capacity=0, tile_rows=0, options=0):
         self._lib = L.lib()
         prec = {"fp64": L.FP64_PLAIN, "plain": L.FP64_PLAIN, "fp32": L.FP32_MIXED, "mixed": L.FP32_MIXED}[precision]
         self.cfg = L.Config(mx=mx, my=my, dx=dx, dy=dy, dt=dt, cva=cva, mime=mime, in0=in0, ybc=ybc,
                             precision=prec, compat=compat, track_pid=int(bool(track_pid)),
-                            capacity=int(capacity), tile_rows=tile_rows)
+                            capacity=int(capacity), tile_rows=tile_rows, options=options)
         self.mx, self.my = mx, my
         self.precision = precision
         self._h = ctypes.c_void_p()
