@@ -9,7 +9,10 @@ Gauss residual max|div E / cva^2 - rho| of each form; the energy history
 (one JSON object) gives, per form, the total-energy drift |E(t)/E(0) - 1| at
 the end and its maximum, the Gauss residuals and the flux series, and the
 differences between the forms: the largest relative difference of the total
-energy and of the flux, and the largest Gauss residual of each form.
+energy and of the flux, and the largest Gauss residual of each form. With
+--control a second FP64 run gives the same differences between two FP64 runs
+(their FP64 atomic sums round in the order the atomics land, so they are not
+bit-identical), the spread that chaotic dynamics alone produce.
 """
 import argparse
 import json
@@ -51,9 +54,25 @@ def run(workload, steps, every, precision, seed_offset=0):
     return out
 
 
-def compare(workload, steps, every):
+def differences(a, b):
+    ea, eb = a["energy_total"], b["energy_total"]
+    rows = min(len(ea), len(eb))
+    rel_e = np.abs(ea[:rows] - eb[:rows]) / np.abs(eb[:rows])
+    fa, fb = np.array(a["flux"]), np.array(b["flux"])
+    scale = max(float(np.max(np.abs(fb))), 1e-300)
+    return {"total_energy_rel_diff_max": float(rel_e.max()),
+            "flux_diff_rel_to_max_flux": [float(x) for x in np.abs(fa - fb) / scale]}
+
+
+def compare(workload, steps, every, control=False):
     m = run(workload, steps, every, "fp32")
     d = run(workload, steps, every, "fp64")
+    extra = {}
+    if control:
+        d2 = run(workload, steps, every, "fp64")
+        extra["fp64_vs_fp64"] = differences(d2, d)
+        extra["fp32_vs_fp64_flux"] = differences(m, d)["flux_diff_rel_to_max_flux"]
+        d2.pop("energy_total")
     em, ed = m.pop("energy_total"), d.pop("energy_total")
     rows = min(len(em), len(ed))
     rel_e = np.abs(em[:rows] - ed[:rows]) / np.abs(ed[:rows])
@@ -66,6 +85,7 @@ def compare(workload, steps, every):
         "total_energy_rel_diff_end": float(rel_e[-1]),
         "flux_diff_max_rel_to_max_flux": float(np.max(np.abs(fm - fd)) / scale),
         "gauss_mixed_max": float(max(m["gauss"])), "gauss_fp64_max": float(max(d["gauss"])),
+        **extra,
     }
 
 
@@ -74,8 +94,9 @@ def main():
     ap.add_argument("--workload", default="harris_1024x512_ppc100", choices=sorted(configs.WORKLOADS))
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--every", type=int, default=500)
+    ap.add_argument("--control", action="store_true", help="a second FP64 run for the chaotic spread")
     args = ap.parse_args()
-    print(json.dumps(compare(args.workload, args.steps, args.every)), flush=True)
+    print(json.dumps(compare(args.workload, args.steps, args.every, args.control)), flush=True)
 
 
 if __name__ == "__main__":
