@@ -25,6 +25,8 @@ module pbpic_gpu
     integer(c_int32_t), parameter :: PBPIC_BC_PERIODIC = 0, PBPIC_BC_CONDUCTING = 1
     integer(c_int32_t), parameter :: PBPIC_FP64_PLAIN = 0, PBPIC_FP32_MIXED = 1
     integer(c_int32_t), parameter :: PBPIC_COMPAT_BORIS = 1, PBPIC_COMPAT_FOLD = 2, PBPIC_COMPAT_RHO = 4
+    integer(c_int32_t), parameter :: PBPIC_OPT_NO_AUTOSORT = 1
+    integer(c_int32_t), parameter :: PBPIC_FILTER_MARDER = 1, PBPIC_FILTER_CERENKOV = 2
 
     type, bind(c) :: pbpic_config
         integer(c_int32_t) :: mx, my
@@ -109,6 +111,58 @@ module pbpic_gpu
             import :: c_int, c_ptr, c_int32_t
             type(c_ptr), value :: h
             integer(c_int32_t), intent(out) :: counts(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_status(h, bits) bind(c, name="pbpic_status") result(ierr)
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), intent(out) :: bits
+            integer(c_int) :: ierr
+        end function
+        function pbpic_gauss_residual(h, r) bind(c, name="pbpic_gauss_residual") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: r
+            integer(c_int) :: ierr
+        end function
+        function pbpic_energy_history(h, out, max_rows, n_rows) bind(c, name="pbpic_energy_history") result(ierr)
+            import :: c_int, c_ptr, c_double, c_int32_t
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: out(*)
+            integer(c_int32_t), value :: max_rows
+            integer(c_int32_t), intent(out) :: n_rows
+            integer(c_int) :: ierr
+        end function
+        ! fieldsinfo / particlesinfo: dir is a NUL-terminated character array
+        function pbpic_dump(h, dir) bind(c, name="pbpic_dump") result(ierr)
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: dir(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_restart(h, dir) bind(c, name="pbpic_restart") result(ierr)
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: dir(*)
+            integer(c_int) :: ierr
+        end function
+        ! divergenceclean / suppresscerenkov (pic2d.f90:867-907)
+        function pbpic_set_field_filters(h, flags, marder_d, cerenkov_tau) &
+                bind(c, name="pbpic_set_field_filters") result(ierr)
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: flags
+            real(c_double), value :: marder_d, cerenkov_tau
+            integer(c_int) :: ierr
+        end function
+        ! energyspectra (pic2d.f90:1957-1990): counts(nbins, 2) in Fortran order
+        function pbpic_energy_spectra(h, de_electron, de_ion, nbins, counts) &
+                bind(c, name="pbpic_energy_spectra") result(ierr)
+            import :: c_int, c_ptr, c_int32_t, c_int64_t, c_double
+            type(c_ptr), value :: h
+            real(c_double), value :: de_electron, de_ion
+            integer(c_int32_t), value :: nbins
+            integer(c_int64_t), intent(out) :: counts(*)
             integer(c_int) :: ierr
         end function
         function pbpic_last_error() bind(c, name="pbpic_last_error") result(msg)

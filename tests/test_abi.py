@@ -88,3 +88,16 @@ def test_batch_create_rejects_bad_domains_before_device_work():
     assert lib.pbpic_batch_create(cfgs, loaders, 1, ctypes.byref(out)) == -1
     assert b"FP32" in lib.pbpic_last_error()
     assert lib.pbpic_batch_create(cfgs, loaders, 0, ctypes.byref(out)) == -1
+
+
+def test_fortran_module_binds_exported_symbols():
+    """Every bind(c) name in the Fortran interface module is a function the
+    library exports (the module cannot be compiled here: no Fortran compiler)."""
+    from pbpic_b200 import build
+    lib = ctypes.CDLL(build.build())
+    src = open(os.path.join(ROOT, "pbpic_b200", "fortran", "pbpic_gpu.f90")).read()
+    names = set(re.findall(r'bind\(c,\s*name="(pbpic_\w+)"\)', src))
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(declared_functions()) | {"pbpic_last_error"}
