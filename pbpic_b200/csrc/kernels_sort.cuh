@@ -97,6 +97,52 @@ static __global__ void k_cell_keys(const uint32_t* cell, int64_t n, int my, int3
   if (ok && (lane_id() == (unsigned)(__ffs(peers) - 1))) atomicAdd(&counts[key], __popc(peers));
 }
 
+// Sort of an array in which every cell's particles form one contiguous run
+// (concatenated cell-sorted pieces with disjoint cells, e.g. a slab's own
+// particles followed by its ghost bands): k_cell_runs counts the run starts
+// of each cell and records the position of one, k_runs_ok flags a cell with
+// more than one run, and k_run_scatter moves each particle to
+// offset(cell) + (its index - the run start), the stable sort's position.
+static __global__ void k_cell_runs(const uint32_t* cell, int64_t n, int my, int32_t* nruns, int32_t* runstart) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = cell[i];
+    const int key = cw_ix(w) * my + cw_iy(w);
+    int prev = -1;
+    if (i > 0) {
+      const uint32_t v = cell[i - 1];
+      prev = cw_ix(v) * my + cw_iy(v);
+    }
+    if (key != prev) {
+      atomicAdd(&nruns[key], 1);
+      runstart[key] = (int32_t)i;
+    }
+  }
+}
+
+static __global__ void k_runs_ok(const int32_t* nruns, int64_t ncells, int* flag) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += (int64_t)gridDim.x * blockDim.x)
+    if (nruns[c] > 1) atomicOr(flag, 1);
+}
+
+template <class T>
+__global__ void k_run_scatter(int64_t n, int my, const int32_t* off, const int32_t* runstart, const uint32_t* ci,
+                              const T* dxi, const T* dyi, const T* uxi, const T* uyi, const T* uzi,
+                              const int32_t* pidi, uint32_t* co, T* dxo, T* dyo, T* uxo, T* uyo, T* uzo,
+                              int32_t* pido) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = ci[i];
+    const int key = cw_ix(w) * my + cw_iy(w);
+    const int64_t d = (int64_t)off[key] + (i - runstart[key]);
+    co[d] = w;
+    dxo[d] = dxi[i];
+    dyo[d] = dyi[i];
+    uxo[d] = uxi[i];
+    uyo[d] = uyi[i];
+    uzo[d] = uzi[i];
+    if (pido) pido[d] = pidi[i];
+  }
+}
+
 // Histogram of caller-provided keys, flagging keys outside [0, ncells).
 static __global__ void k_key_hist(const int32_t* keys, int64_t n, int32_t ncells, int32_t* counts, int* status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

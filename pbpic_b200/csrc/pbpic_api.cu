@@ -173,6 +173,7 @@ struct pbpic_handle {
   int filters = 0;               // field filters (PBPIC_FILTER_*), periodic y only
   double marder_d = 0.001, cer_tau = 0.125;
   void* fc = nullptr;            // filter corrections, 5 x mx x my values of the precision
+  int32_t* runbuf = nullptr;        // run-merge sort: run counts and run starts (2 x cells)
   int32_t* band_flags = nullptr;    // slab exchange: flags / positions (capacity + 2)
   int32_t* band_scratch = nullptr;  // and their scan's chunk totals
   std::vector<void*> allocs;
@@ -374,7 +375,33 @@ int do_sort(pbpic_handle* h) {
   }
   CK(cudaMemcpyAsync(h->off, h->counts, (size_t)(h->ncells + 1) * 4, cudaMemcpyDeviceToDevice, s));
   TRY(scan_excl(s, h->off, h->ncells + 1, h->scan_scratch));
+  // one run per cell (concatenated sorted pieces): a single scatter suffices
+  bool runs = false;
   if (n > 0) {
+    if (!h->runbuf) TRY(dalloc(h, &h->runbuf, ((size_t)2 * h->ncells + 16) * 4));
+    int32_t* nruns = h->runbuf;
+    int32_t* runstart = h->runbuf + h->ncells;
+    int* flag = (int*)(h->runbuf + 2 * (size_t)h->ncells);
+    CK(cudaMemsetAsync(nruns, 0, (size_t)h->ncells * 4, s));
+    CK(cudaMemsetAsync(flag, 0, 4, s));
+    k_cell_runs<<<grid_for(n, 256), 256, 0, s>>>(h->cell[b], n, h->cfg.my, nruns, runstart);
+    CKLAUNCH("k_cell_runs");
+    k_runs_ok<<<grid_for(h->ncells, 256), 256, 0, s>>>(nruns, h->ncells, flag);
+    CKLAUNCH("k_runs_ok");
+    int many = 1;
+    CK(cudaMemcpyAsync(&many, flag, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (!many) {
+      k_run_scatter<T><<<grid_for(n, 256), 256, 0, s>>>(n, h->cfg.my, h->off, runstart, h->cell[b], P<T>(h, b, 0),
+                                                        P<T>(h, b, 1), P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4),
+                                                        h->pid[b], h->cell[o], P<T>(h, o, 0), P<T>(h, o, 1),
+                                                        P<T>(h, o, 2), P<T>(h, o, 3), P<T>(h, o, 4), h->pid[o]);
+      CKLAUNCH("k_run_scatter");
+      h->cur = o;
+      runs = true;
+    }
+  }
+  if (n > 0 && !runs) {
     int32_t* perm = nullptr;
     TRY(radix_sort(s, n, h->ncells, h->keys[0], h->keys[1], h->vals[0], h->vals[1], h->rhist, h->scan_scratch,
                    &perm));

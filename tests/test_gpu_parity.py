@@ -303,3 +303,26 @@ def test_fused_sort_is_the_stable_sort(gpu_lib, oracle_mod, precision, ybc, mx, 
                 assert np.array_equal(post[c], pre[c][order])
             assert np.array_equal(s.cell_counts(), np.bincount(pre["grid"] - 1, minlength=mx * my))
         assert s.status() == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_sort_of_whole_cell_runs(gpu_lib, oracle_mod, precision):
+    """Particles whose cells each form one contiguous run, the runs in shuffled
+    order (as after a slab exchange: sorted pieces with disjoint cells), sort
+    by the single-scatter path to the stable counting sort's order."""
+    cfg, ld, p, _ = plasma(oracle_mod, 0, mx=16, my=12, ppc=6)
+    o = oracle_mod.Oracle(**cfg)
+    o.load_particles(p)
+    o.countingsort()
+    ps = o.particles()
+    starts = np.flatnonzero(np.r_[True, ps["grid"][1:] != ps["grid"][:-1]])
+    runs = np.split(ps, starts[1:])
+    rng = np.random.default_rng(9)
+    q = np.concatenate([runs[k] for k in rng.permutation(len(runs))])
+    assert not np.array_equal(q["pid"], ps["pid"])
+    with new_sim(cfg, len(q), precision=precision) as s:
+        s.load_particles(q)
+        s.countingsort()
+        got = s.particles()
+        assert np.array_equal(got["pid"], ps["pid"])
+        assert np.array_equal(s.cell_counts(), np.bincount(ps["grid"] - 1, minlength=cfg["mx"] * cfg["my"]))
