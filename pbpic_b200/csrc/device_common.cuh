@@ -6,7 +6,7 @@
 namespace pbd {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int NTHREADS = 256;  // threads per block of the particle kernels
+constexpr int NTHREADS = 128;  // threads per block of the push (4 blocks of 128 per SM: finer passes than 2 of 256)
 
 // Current components (denjr record of pic2d.f90:65-67).
 enum { JX = 0, JY = 1, JZ = 2, RHO = 3 };

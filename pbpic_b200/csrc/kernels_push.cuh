@@ -419,7 +419,7 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 #define PBPIC_PUSH_UNROLL 0
 #endif
 #ifndef PBPIC_PUSH_MINBLOCKS
-#define PBPIC_PUSH_MINBLOCKS 2
+#define PBPIC_PUSH_MINBLOCKS 4
 #endif
 #ifndef PBPIC_PUSH_NODECACHE
 #define PBPIC_PUSH_NODECACHE 0
