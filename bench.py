@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy error"
 # DRAM bytes per particle of one k_push launch (read + write) from the ncu capture summarised in
 # profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to the particles.
-PUSH_DRAM_BYTES_PER_PARTICLE = 50.3
+PUSH_DRAM_BYTES_PER_PARTICLE = 48.6
 UNIT = "particle-steps/s"
 
 

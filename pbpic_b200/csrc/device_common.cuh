@@ -6,7 +6,15 @@
 namespace pbd {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int NTHREADS = 128;  // threads per block of the push (4 blocks of 128 per SM: finer passes than 2 of 256)
+constexpr int NTHREADS = 256;  // threads per block of the particle kernels
+
+// Threads per block of the push: FP32 (mixed) 128, four blocks per SM (finer
+// passes over a tile than two blocks of 256, 1.4 % faster step); FP64 (plain,
+// about 210 registers) 256, which keeps two resident blocks' worth of warps.
+template <class T>
+struct PushThreads {
+  static constexpr int value = sizeof(T) == 4 ? 128 : 256;
+};
 
 // Current components (denjr record of pic2d.f90:65-67).
 enum { JX = 0, JY = 1, JZ = 2, RHO = 3 };

@@ -427,7 +427,7 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 
 template <class T>
 struct PushSmem {
-  T stage[NTHREADS / 32][17][33];  // per-warp transposition of the stencil sums
+  T stage[PushThreads<T>::value / 32][17][33];  // per-warp transposition of the stencil sums
   double red[32];
 };
 
@@ -510,7 +510,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   T* mycol = &sm.stage[w][0][lane];
   double ke_e = 0.0, ke_i = 0.0;
   int status = 0;
-  for (int q0 = pbeg & ~3; q0 < pend; q0 += PT * NTHREADS) {
+  for (int q0 = pbeg & ~3; q0 < pend; q0 += PT * PushThreads<T>::value) {
     // thread-level accumulation of the stencils of particles sharing a cell
     T acc[17];
 #pragma unroll
@@ -758,7 +758,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 
 // Single domain: one block per tile.
 template <class T, bool MIXED, bool HIST>
-__global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
+__global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T> sm;
   push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES>(a, blockIdx.x, sm, smem_raw);
@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_
 // Batched domains: persistent blocks take (domain, tile) pairs from a global
 // counter (reset to 0 before each launch) in the order of `tiles`.
 template <class T, bool MIXED, bool HIST, int G>
-__global__ void __launch_bounds__(NTHREADS, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
+__global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
     k_push_batched(const PushParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T> sm;

@@ -430,8 +430,9 @@ int do_push(pbpic_handle* h) {
   PushParams<T> p = push_params<T, MIXED>(h);
   const size_t smem = push_smem_bytes(h->TY, MIXED);
   const bool hist = h->sorted && h->fused_ok;
-  if (hist) k_push<T, MIXED, true><<<h->ntiles, NTHREADS, smem, s>>>(p);
-  else k_push<T, MIXED, false><<<h->ntiles, NTHREADS, smem, s>>>(p);
+  const int nt = PushThreads<T>::value;
+  if (hist) k_push<T, MIXED, true><<<h->ntiles, nt, smem, s>>>(p);
+  else k_push<T, MIXED, false><<<h->ntiles, nt, smem, s>>>(p);
   CKLAUNCH("k_push");
   k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
   CKLAUNCH("k_energy_row");
@@ -1485,9 +1486,9 @@ int batch_layout(pbpic_batch* b) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   int per_sm = 1;
   if (b->groups == 1) {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 1>, NTHREADS, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 1>, PushThreads<float>::value, smem));
   } else {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 2>, NTHREADS, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 2>, PushThreads<float>::value, smem));
   }
   b->push_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_scatter_batched<float>, 256, 0));
@@ -1600,9 +1601,9 @@ int batch_enqueue_step(pbpic_batch* b, int par) {
   CKLAUNCH("k_batch_begin");
   const PushParams<float>* pp = b->d_push + (size_t)par * D;
   if (b->groups == 1)
-    k_push_batched<float, true, true, 1><<<b->push_blocks, NTHREADS, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 1><<<b->push_blocks, PushThreads<float>::value, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   else
-    k_push_batched<float, true, true, 2><<<b->push_blocks, NTHREADS, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 2><<<b->push_blocks, PushThreads<float>::value, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   CKLAUNCH("k_push_batched");
   k_fused_counts_batched<<<dim3(b->gx_cells, D), 256, 0, s>>>(b->d_fsort);
   CKLAUNCH("k_fused_counts_batched");
