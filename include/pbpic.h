@@ -51,6 +51,7 @@ extern "C" {
 #define PBPIC_STATUS_CELL_JUMP 1 /* a particle moved more than one cell in a step (pic2d.f90:1008-1023 assumes at most one) */
 #define PBPIC_STATUS_NAN 2       /* a momentum became NaN or infinite */
 #define PBPIC_STATUS_UNSORTED 4  /* a push met a particle outside its tile (informational) */
+#define PBPIC_STATUS_BAD_RECORD 8   /* a band record fell outside this domain's rows (pbpic_band_replace) */
 #define PBPIC_STATUS_COPY_TIMEOUT 16 /* a bulk copy into shared memory did not complete within 2 s (the step's results are invalid) */
 
 typedef struct pbpic_config {
@@ -280,6 +281,12 @@ int pbpic_band_extract(pbpic_handle* h, int32_t y_lo, int32_t y_hi, int32_t my_g
 int pbpic_band_keep(pbpic_handle* h, int32_t y_lo, int32_t y_hi);
 /* Appends n records from device memory; local row = global row - row_offset. */
 int pbpic_band_append(pbpic_handle* h, const void* src_dev, int64_t n, int32_t my_global, int32_t row_offset);
+/* pbpic_band_keep(y_lo, y_hi), then both appends, then a sort, in one pass
+ * when the particles are sorted by cell: the bands (device records, each in
+ * the cell order band_extract produced) go below (bottom, local row = global
+ * row - off_bottom) and above (top) the own rows. Leaves the particles sorted. */
+int pbpic_band_replace(pbpic_handle* h, int32_t y_lo, int32_t y_hi, const void* bottom_dev, int64_t nb,
+                       int32_t off_bottom, const void* top_dev, int64_t nt, int32_t off_top, int32_t my_global);
 /* Rows j0 .. j0+nrows-1 of the six field planes to / from device memory as
  * [6][mx][nrows] values of the handle's precision; setting them recomputes
  * the node averages. */

@@ -116,6 +116,7 @@ SIGNATURES = {
     "pbpic_band_extract": [_P, _I32, _I32, _I32, _I32, _P, _I64, _PI64],
     "pbpic_band_keep": [_P, _I32, _I32],
     "pbpic_band_append": [_P, _P, _I64, _I32, _I32],
+    "pbpic_band_replace": [_P, _I32, _I32, _P, _I64, _I32, _P, _I64, _I32, _I32],
     "pbpic_field_rows_get": [_P, _I32, _I32, _P],
     "pbpic_field_rows_set": [_P, _I32, _I32, _P],
     "pbpic_energies_rows": [_P, _I32, _I32, _I32, _I32, _P],

@@ -9,6 +9,10 @@
 //   k_band_in                    reference records (global grid) -> appended
 //   k_rows_get / k_rows_set      rows of the six field planes
 //   k_kinetic_rows, k_field_energy_rows   energy sums over the own rows
+// and, when the particles are sorted by cell, single-pass versions: a band
+// copied column by column from the cell offsets (k_band_out_sorted), and the
+// own rows merged with both received bands straight into cell order
+// (k_band_assemble).
 #pragma once
 #include "device_common.cuh"
 #include "kernels_misc.cuh"
@@ -169,6 +173,134 @@ __global__ void k_field_energy_rows(int mx, int my, const T* ng, int y_lo, int y
   if (threadIdx.x == 0) {
     part[2 * blockIdx.x] = se;
     part[2 * blockIdx.x + 1] = sb;
+  }
+}
+
+}  // namespace pbd
+
+namespace pbd {
+
+// ----------------------------------------------- sorted fast paths of the slab
+// When the particles are sorted by cell, the particles of rows [y_lo, y_hi)
+// of column ix are the range [off[ix*my + y_lo], off[ix*my + y_hi]).
+
+// Per column: the number of particles of rows [y_lo, y_hi) (colcnt[mx] = 0).
+static __global__ void k_col_counts(const int32_t* off, int mx, int my, int y_lo, int y_hi, int32_t* colcnt) {
+  for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix <= mx; ix += gridDim.x * blockDim.x)
+    colcnt[ix] = ix == mx ? 0 : off[(int64_t)ix * my + y_hi] - off[(int64_t)ix * my + y_lo];
+}
+
+// Column of output index k: the last ix with start[ix] <= k (start: exclusive
+// scan over mx columns, start[mx] = total).
+__device__ __forceinline__ int column_of(const int32_t* start, int mx, int64_t k) {
+  int lo = 0, hi = mx - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= k) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Band extraction from sorted particles: output k of column ix comes from
+// off[ix*my + y_lo] + (k - colstart[ix]); same records as k_band_out.
+template <class T, class R>
+__global__ void k_band_out_sorted(int64_t total, const int32_t* colstart, const int32_t* off, int mx, int my, int y_lo,
+                                  const uint32_t* cell, const T* dx, const T* dy, const T* ux, const T* uy,
+                                  const T* uz, const int32_t* pid, int my_global, int row_offset, RefRec<R>* out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = column_of(colstart, mx, k);
+    const int64_t i = (int64_t)off[(int64_t)ix * my + y_lo] + (k - colstart[ix]);
+    const uint32_t w = cell[i];
+    RefRec<R> r;
+    r.dx = (R)dx[i];
+    r.dy = (R)dy[i];
+    r.ux = (R)ux[i];
+    r.uy = (R)uy[i];
+    r.uz = (R)uz[i];
+    r.grid = my_global * cw_ix(w) + cw_iy(w) + row_offset + 1;
+    r.q = cw_sp(w) ? -1 : 1;
+    r.pid = pid ? pid[i] : 0;
+    out[k] = r;
+  }
+}
+
+// Particles per output column: bottom band + own rows + top band.
+static __global__ void k_col_sum3(const int32_t* a, const int32_t* b, const int32_t* c, int mx, int32_t* out) {
+  for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix <= mx; ix += gridDim.x * blockDim.x)
+    out[ix] = ix == mx ? 0 : a[ix] + b[ix] + c[ix];
+}
+
+// Per-column counts of band records (global grid) that come in column order:
+// the first and one-past-last record of each column's run are found at the
+// run boundaries (no atomics: neighbouring threads share a column), then
+// cnt = last - first (both zero for an absent column).
+template <class R>
+__global__ void k_band_col_bounds(const RefRec<R>* in, int64_t n, int my_global, int mx, int32_t* first,
+                                  int32_t* last) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (in[i].grid - 1) / my_global;
+    if (ix < 0 || ix >= mx) continue;
+    const int prev = i > 0 ? (in[i - 1].grid - 1) / my_global : -1;
+    const int next = i + 1 < n ? (in[i + 1].grid - 1) / my_global : -1;
+    if (prev != ix) first[ix] = (int32_t)i;
+    if (next != ix) last[ix] = (int32_t)(i + 1);
+  }
+}
+
+static __global__ void k_col_diff(const int32_t* first, const int32_t* last, int mx, int32_t* cnt) {
+  for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix <= mx; ix += gridDim.x * blockDim.x)
+    cnt[ix] = ix == mx ? 0 : last[ix] - first[ix];
+}
+
+// The slab's new particle array in cell order, column by column: the bottom
+// band's particles of the column, the own rows' particles (sorted input,
+// range from off), the top band's particles. Band records are in column order
+// and, within a column, in cell order (they were extracted that way).
+struct ReplaceSrc {
+  const int32_t* off;      // cell offsets of the sorted input
+  const int32_t* outstart; // [mx + 1] first output position of each column
+  const int32_t* bstart;   // [mx + 1] first bottom-band record of each column
+  const int32_t* bcnt;     // [mx] bottom-band records per column
+  const int32_t* ocnt;     // [mx] own particles per column
+  int mx, my, y_lo, my_global, off_bottom, off_top;
+  const int32_t* tstart;   // [mx + 1] first top-band record of each column
+};
+
+template <class T, class R>
+__global__ void k_band_assemble(int64_t total, ReplaceSrc s, const RefRec<R>* bot, const RefRec<R>* top,
+                                const uint32_t* ci, const T* dxi, const T* dyi, const T* uxi, const T* uyi,
+                                const T* uzi, const int32_t* pidi, uint32_t* co, T* dxo, T* dyo, T* uxo, T* uyo,
+                                T* uzo, int32_t* pido, int* status) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = column_of(s.outstart, s.mx, k);
+    int64_t r = k - s.outstart[ix];
+    const int nb = s.bcnt[ix], no = s.ocnt[ix];
+    if (r >= nb && r < nb + no) {  // own particle
+      const int64_t i = (int64_t)s.off[(int64_t)ix * s.my + s.y_lo] + (r - nb);
+      co[k] = ci[i];
+      dxo[k] = dxi[i];
+      dyo[k] = dyi[i];
+      uxo[k] = uxi[i];
+      uyo[k] = uyi[i];
+      uzo[k] = uzi[i];
+      if (pido) pido[k] = pidi[i];
+      continue;
+    }
+    const bool lower = r < nb;
+    const RefRec<R> rec = lower ? bot[s.bstart[ix] + r] : top[s.tstart[ix] + (r - nb - no)];
+    const int g = rec.grid - 1;
+    const int gx = g / s.my_global, gy = g - gx * s.my_global;
+    const int iy = gy - (lower ? s.off_bottom : s.off_top);
+    const bool ok = gx == ix && iy >= 0 && iy < s.my && (rec.q == 1 || rec.q == -1);
+    if (!ok) atomicOr(status, 8);
+    co[k] = ok ? cw_make(ix, iy, rec.q < 0 ? 1 : 0) : cw_make(ix, s.y_lo, 1);
+    dxo[k] = ok ? (T)rec.dx : T(0);
+    dyo[k] = ok ? (T)rec.dy : T(0);
+    uxo[k] = ok ? (T)rec.ux : T(0);
+    uyo[k] = ok ? (T)rec.uy : T(0);
+    uzo[k] = ok ? (T)rec.uz : T(0);
+    if (pido) pido[k] = rec.pid;
   }
 }
 

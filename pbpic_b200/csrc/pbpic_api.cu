@@ -176,6 +176,8 @@ struct pbpic_handle {
   int32_t* runbuf = nullptr;        // run-merge sort: run counts and run starts (2 x cells)
   int32_t* band_flags = nullptr;    // slab exchange: flags / positions (capacity + 2)
   int32_t* band_scratch = nullptr;  // and their scan's chunk totals
+  int32_t* colbuf = nullptr;        // sorted slab paths: per-column counts and starts (8 x (mx + 1))
+  int32_t* colscan = nullptr;       // and their scans' chunk totals
   std::vector<void*> allocs;
 };
 
@@ -2075,9 +2077,44 @@ int band_positions(pbpic_handle* h, int y_lo, int y_hi, int64_t* count) {
   return PBPIC_OK;
 }
 
+int col_buffers(pbpic_handle* h) {
+  if (h->colbuf) return PBPIC_OK;
+  TRY(dalloc(h, &h->colbuf, (size_t)8 * (h->cfg.mx + 1) * 4));
+  TRY(dalloc(h, &h->colscan, (size_t)scan_scratch_ints(h->cfg.mx + 1) * 4));
+  return PBPIC_OK;
+}
+
+// Particles sorted by cell: a band of rows is one range per column (cell offsets).
+template <class T, bool MIXED>
+int band_extract_sorted(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_offset, void* dst, int64_t cap,
+                        int64_t* nout) {
+  TRY(col_buffers(h));
+  cudaStream_t s = h->stream;
+  const int mx = h->cfg.mx;
+  int32_t* colstart = h->colbuf;
+  k_col_counts<<<grid_for(mx + 1, 256), 256, 0, s>>>(h->off, mx, h->cfg.my, y_lo, y_hi, colstart);
+  CKLAUNCH("k_col_counts");
+  TRY(scan_excl(s, colstart, mx + 1, h->colscan));
+  int32_t total = 0;
+  CK(cudaMemcpyAsync(&total, colstart + mx, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (nout) *nout = total;
+  if (total > cap) return fail(PBPIC_ECAPACITY, "the band holds more particles than the destination");
+  const int b = h->cur;
+  if (total > 0) {
+    k_band_out_sorted<T, T><<<grid_for(total, 256), 256, 0, s>>>(
+        total, colstart, h->off, mx, h->cfg.my, y_lo, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
+        P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], my_global, row_offset, (RefRec<T>*)dst);
+    CKLAUNCH("k_band_out_sorted");
+  }
+  CK(cudaStreamSynchronize(s));
+  return PBPIC_OK;
+}
+
 template <class T, bool MIXED>
 int do_band_extract(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_offset, void* dst, int64_t cap,
                     int64_t* nout) {
+  if (h->sorted) return band_extract_sorted<T, MIXED>(h, y_lo, y_hi, my_global, row_offset, dst, cap, nout);
   int64_t c = 0;
   TRY(band_positions(h, y_lo, y_hi, &c));
   if (nout) *nout = c;
@@ -2130,6 +2167,89 @@ int do_band_append(pbpic_handle* h, const void* src, int64_t n, int my_global, i
   h->n += n;
   TRY(set_unsorted_tiles(h));
   if (st & 8) return fail(PBPIC_EINVAL, "band record outside this domain's rows or with q not +-1");
+  return PBPIC_OK;
+}
+
+// Own rows [y_lo, y_hi) plus the two received bands, in cell order, in one
+// pass (particles sorted by cell on entry); otherwise compaction, appends and
+// a sort.
+template <class T, bool MIXED>
+int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_t nb, int off_bottom,
+                    const void* top, int64_t nt, int off_top, int my_global) {
+  if (!h->sorted) {
+    TRY((do_band_keep<T, MIXED>(h, y_lo, y_hi)));
+    TRY((do_band_append<T, MIXED>(h, bot, nb, my_global, off_bottom)));
+    TRY((do_band_append<T, MIXED>(h, top, nt, my_global, off_top)));
+    return do_sort<T, MIXED>(h);
+  }
+  if ((nb && !bot) || (nt && !top) || nb < 0 || nt < 0) return fail(PBPIC_EINVAL, "null or negative band");
+  TRY(col_buffers(h));
+  cudaStream_t s = h->stream;
+  const int mx = h->cfg.mx, my = h->cfg.my;
+  const size_t m1 = (size_t)mx + 1;
+  int32_t *ocnt = h->colbuf, *bcnt = ocnt + m1, *tcnt = bcnt + m1, *bstart = tcnt + m1, *tstart = bstart + m1,
+          *outstart = tstart + m1;
+  k_col_counts<<<grid_for(mx + 1, 256), 256, 0, s>>>(h->off, mx, my, y_lo, y_hi, ocnt);
+  CKLAUNCH("k_col_counts");
+  int32_t *first = outstart + m1, *last = first + m1;
+  for (int band = 0; band < 2; ++band) {  // per-column counts of the bands (column-ordered records)
+    const void* src = band == 0 ? bot : top;
+    const int64_t nr = band == 0 ? nb : nt;
+    int32_t* cnt = band == 0 ? bcnt : tcnt;
+    CK(cudaMemsetAsync(first, 0, 2 * m1 * 4, s));
+    if (nr) {
+      k_band_col_bounds<T><<<grid_for(nr, 256), 256, 0, s>>>((const RefRec<T>*)src, nr, my_global, mx, first, last);
+      CKLAUNCH("k_band_col_bounds");
+    }
+    k_col_diff<<<grid_for(mx + 1, 256), 256, 0, s>>>(first, last, mx, cnt);
+    CKLAUNCH("k_col_diff");
+  }
+  CK(cudaMemcpyAsync(bstart, bcnt, 2 * m1 * 4, cudaMemcpyDeviceToDevice, s));  // bstart, tstart
+  k_col_sum3<<<grid_for(mx + 1, 256), 256, 0, s>>>(ocnt, bcnt, tcnt, mx, outstart);
+  CKLAUNCH("k_col_sum3");
+  TRY(scan_excl(s, bstart, (int64_t)m1, h->colscan));
+  TRY(scan_excl(s, tstart, (int64_t)m1, h->colscan));
+  TRY(scan_excl(s, outstart, (int64_t)m1, h->colscan));
+  int32_t total = 0;
+  CK(cudaMemcpyAsync(&total, outstart + mx, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (total > h->cap) return fail(PBPIC_ECAPACITY, "the slab's particles and bands exceed the capacity");
+  const int b = h->cur, o = 1 - b;
+  ReplaceSrc rs;
+  rs.off = h->off;
+  rs.outstart = outstart;
+  rs.bstart = bstart;
+  rs.bcnt = bcnt;
+  rs.ocnt = ocnt;
+  rs.mx = mx;
+  rs.my = my;
+  rs.y_lo = y_lo;
+  rs.my_global = my_global;
+  rs.off_bottom = off_bottom;
+  rs.off_top = off_top;
+  rs.tstart = tstart;
+  if (total > 0) {
+    k_band_assemble<T, T><<<grid_for(total, 256), 256, 0, s>>>(
+        total, rs, (const RefRec<T>*)bot, (const RefRec<T>*)top, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
+        P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], h->cell[o], P<T>(h, o, 0), P<T>(h, o, 1),
+        P<T>(h, o, 2), P<T>(h, o, 3), P<T>(h, o, 4), h->pid[o], h->status);
+    CKLAUNCH("k_band_assemble");
+  }
+  h->cur = o;
+  h->n = total;
+  // cell offsets and tile ranges of the new (sorted) array
+  CK(cudaMemsetAsync(h->counts, 0, (size_t)(h->ncells + 1) * 4, s));
+  if (total > 0) {
+    k_cell_keys<<<(unsigned)(((int64_t)total + 255) / 256), 256, 0, s>>>(h->cell[o], total, my, nullptr, h->counts);
+    CKLAUNCH("k_cell_keys");
+  }
+  CK(cudaMemcpyAsync(h->off, h->counts, (size_t)(h->ncells + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  TRY(scan_excl(s, h->off, h->ncells + 1, h->scan_scratch));
+  k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, my, total,
+                                                                  h->tile_off);
+  CKLAUNCH("k_tile_off");
+  h->sorted = true;
+  h->hist_valid = false;
   return PBPIC_OK;
 }
 
@@ -2193,6 +2313,13 @@ int pbpic_band_append(pbpic_handle* h, const void* src_dev, int64_t n, int32_t m
   TRY(check_handle(h));
   if (my_global < 1) return fail(PBPIC_EINVAL, "bad global row count");
   return DISPATCH(h, do_band_append, h, src_dev, n, my_global, row_offset);
+}
+
+int pbpic_band_replace(pbpic_handle* h, int32_t y_lo, int32_t y_hi, const void* bottom_dev, int64_t nb,
+                       int32_t off_bottom, const void* top_dev, int64_t nt, int32_t off_top, int32_t my_global) {
+  TRY(check_handle(h));
+  if (y_lo < 0 || y_hi > h->cfg.my || y_lo > y_hi || my_global < 1) return fail(PBPIC_EINVAL, "bad band rows");
+  return DISPATCH(h, do_band_replace, h, y_lo, y_hi, bottom_dev, nb, off_bottom, top_dev, nt, off_top, my_global);
 }
 
 int pbpic_field_rows_get(pbpic_handle* h, int32_t j0, int32_t nrows, void* dst_dev) {

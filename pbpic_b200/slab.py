@@ -13,7 +13,8 @@ refreshed every step:
 
   1. push and field solve on every slab;
   2. particles: each slab drops everything outside its own rows and receives
-     its neighbours' particles within G rows of the boundary as ghosts. A
+     its neighbours' particles within G rows of the boundary as ghosts (on the
+     GPU one pass that writes the own rows and both bands in cell order). A
      particle that crosses a slab boundary was pushed, bit for bit, by both
      slabs (as an own particle on one side, a ghost on the other: same state,
      same fields); it now sits in the other slab's own rows and is kept
@@ -95,6 +96,15 @@ class GpuEngine:
 
     def keep(self, y_lo, y_hi):
         L.check(self.lib.pbpic_band_keep(self.sim.handle, y_lo, y_hi))
+
+    def replace(self, y_lo, y_hi, bottom, off_bottom, top, off_top):
+        """Own rows plus both received bands, in cell order, in one pass."""
+        n_b = 0 if bottom is None else bottom.numel() // self.rec.itemsize
+        n_t = 0 if top is None else top.numel() // self.rec.itemsize
+        p_b = ctypes.c_void_p(bottom.contiguous().data_ptr()) if n_b else None
+        p_t = ctypes.c_void_p(top.contiguous().data_ptr()) if n_t else None
+        L.check(self.lib.pbpic_band_replace(self.sim.handle, y_lo, y_hi, p_b, n_b, off_bottom, p_t, n_t, off_top,
+                                            self.lay.my))
 
     def append(self, band, row_offset):
         n = band.numel() // self.rec.itemsize
@@ -221,12 +231,8 @@ class SlabRun:
         inc = self.t.exchange(self.slabs, out)
         for r, e in self.slabs.items():
             lay = e.lay
-            e.keep(lay.lo, lay.hi)
             from_down, from_up = inc[r]
-            if from_down is not None:
-                e.append(from_down, lay.off_down)
-            if from_up is not None:
-                e.append(from_up, lay.off_up)
+            e.replace(lay.lo, lay.hi, from_down, lay.off_down, from_up, lay.off_up)
         # fields: own rows next to the neighbours into their ghost rows
         out = {}
         for r, e in self.slabs.items():
@@ -245,6 +251,8 @@ class SlabRun:
 
     def start(self):
         """Fill the ghost bands of freshly loaded slabs and sort."""
+        for e in self.slabs.values():
+            e.sort()  # bands leave in cell order
         self.exchange()
         for e in self.slabs.values():
             e.sort()

@@ -36,6 +36,13 @@ class OracleEngine:
         _, iy = self._rows(p)
         self.o.load_particles(p[(iy >= y_lo) & (iy < y_hi)], capacity=4 * len(p) + 64)
 
+    def replace(self, y_lo, y_hi, bottom, off_bottom, top, off_top):
+        self.keep(y_lo, y_hi)
+        if bottom is not None:
+            self.append(bottom, off_bottom)
+        if top is not None:
+            self.append(top, off_top)
+
     def append(self, band, row_offset):
         q = band.numpy().view(self.O.PARTICLE).copy()
         if len(q) == 0:
