@@ -14,10 +14,14 @@
 // segment in the old cell and one in the new cell. Everything attached to the
 // old cell -- the first segment's jx/jy (and the second's when the particle
 // does not cross), jz on the 3x3 nodes around the cell, rho -- forms a
-// 17-value stencil. Threads of a warp that share a cell are summed by a
-// segmented scan, and the sum of each run is added to a shared-memory window
-// by 17 lanes at once. A crossing particle adds its second segment (4 values)
-// on its own. The window (4 node columns x tile_rows + 3 node rows) is folded
+// 17-value stencil. At the end of a pass the lanes of a warp that share a
+// cell (a run of lanes: the keys do not decrease across a sorted array) are
+// summed: mixed form, each lane stages its stencil in shared memory and 17
+// lanes add up the run's columns in lane order, one stencil entry each (a
+// thread whose particles change cell keeps its first cell's part in a second
+// column, joined to the run it continues); plain form, a segmented scan across
+// the lanes. Each run's sum is added to a shared-memory window by 17 lanes at
+// once. A crossing particle adds its second segment (4 values) on its own. The window (4 node columns x tile_rows + 3 node rows) is folded
 // into the global current at the end, with the periodic wrap and the wall
 // images. Particles outside their tile (array not sorted) add straight to
 // global memory.
@@ -34,7 +38,9 @@
 //
 // With HIST the kernel also counts the new cells of its particles in the
 // tile's window (the 3x3 neighbourhood of the tile), the first half of the
-// fused counting sort (kernels_sort.cuh).
+// fused counting sort (kernels_sort.cuh). The input is sorted, so the counts
+// start from its cell counts (cell_off) and only a crossing particle moves a
+// count, from its old cell's bin to its new one.
 #pragma once
 #include <type_traits>
 #include "device_common.cuh"
@@ -51,6 +57,7 @@ struct PushParams {
   const T* ng;      // node fields (mx+1) x (my+1) x 8: ex ey ez 0 bx by bz 0
   void* jacc;       // 4 planes (jx, jy, jz, rho) of mx x S accumulators
   int32_t* tilecnt; // [ntiles][3*(tile_rows+2)] new-cell counts (HIST)
+  const int32_t* cell_off;  // [mx*my + 1] cell offsets of the sorted input (HIST)
   T c0[2], c1[2], ms[2], qx[2], qy[2], q[2];  // per species: 0 ion, 1 electron
   T dtcva, idx, idy, cva;
   double* ke_part;  // [ntiles][2]: electron, ion kinetic energy of the tile
@@ -425,9 +432,18 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 #define PBPIC_PUSH_NODECACHE 0
 #endif
 
-template <class T>
+// Per-warp staging of the lanes' stencil sums (stride 33: conflict-free rows
+// and columns). The mixed form keeps a second column per lane for the first
+// cell of a lane whose particles change cell inside a pass.
+template <class T, bool MIXED>
 struct PushSmem {
-  T stage[PushThreads<T>::value / 32][17][33];  // per-warp transposition of the stencil sums
+  T stage[PushThreads<T>::value / 32][17][33];
+  double red[32];
+};
+template <>
+struct PushSmem<float, true> {
+  float stage[PushThreads<float>::value / 32][17][33];
+  float first[PushThreads<float>::value / 32][17][33];
   double red[32];
 };
 
@@ -462,23 +478,22 @@ __device__ __noinline__ void flush_column(typename std::conditional<MIXED, long 
   }
 }
 
+// The loop over the 4 particles of a group is not unrolled: each iteration
+// takes element 0 and appends its result, so after 4 iterations the group
+// holds the 4 results in order.
 template <class V>
-__device__ __forceinline__ V pick4(const V (&v)[4], int j) {
-  return j == 0 ? v[0] : (j == 1 ? v[1] : (j == 2 ? v[2] : v[3]));
-}
-template <class V>
-__device__ __forceinline__ void put4(V (&v)[4], int j, V x) {
-  v[0] = j == 0 ? x : v[0];
-  v[1] = j == 1 ? x : v[1];
-  v[2] = j == 2 ? x : v[2];
-  v[3] = j == 3 ? x : v[3];
+__device__ __forceinline__ void rot4(V (&v)[4], V x) {
+  v[0] = v[1];
+  v[1] = v[2];
+  v[2] = v[3];
+  v[3] = x;
 }
 
 // Push of tile t of the domain `a`, by all threads of the block. G float4
 // groups of particles per thread per pass (8 particles for G = 2).
 // smem_raw: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
 template <class T, bool MIXED, bool HIST, int G>
-__device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T>& sm,
+__device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
                                           unsigned char* smem_raw) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
   constexpr int PT = 4 * G;  // particles per thread per pass
@@ -496,8 +511,19 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
       clo[e] = 0u;
       chi[e] = 0;
     }
+  // The input is sorted by cell, so every particle of a tile cell stays in
+  // that cell's bin unless it crosses: the counts start from the input's cell
+  // counts and each crossing particle moves one count.
   if (HIST)
-    for (int e = threadIdx.x; e < NB; e += blockDim.x) hist[e] = 0;
+    for (int e = threadIdx.x; e < NB; e += blockDim.x) {
+      const int by = e - (TY + 2);
+      int v = 0;
+      if (by >= 1 && by <= y1 - y0) {
+        const long long c = (long long)ixt * a.my + y0 + by - 1;
+        v = a.cell_off[c + 1] - a.cell_off[c];
+      }
+      hist[e] = v;
+    }
   __syncthreads();
   Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
@@ -516,6 +542,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 #pragma unroll
     for (int k = 0; k < 17; ++k) acc[k] = T(0);
     int acc_key = -1;
+    int first_key = -1;  // mixed form: cell of this pass's finished first part (in sm.first), or -1
     int cache_cell = -1;
     Node6<T> n00{}, n01{}, n10{}, n11{};
     T pke_e = T(0), pke_i = T(0);  // this pass's kinetic energy, per species
@@ -545,7 +572,6 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           puz[j] = act ? a.uz[p] : T(0);
         }
       }
-      int bins[4] = {-1, -1, -1, -1};
 #if PBPIC_PUSH_UNROLL
 #pragma unroll
 #else
@@ -553,8 +579,16 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 #endif
       for (int j = 0; j < 4; ++j) {
         const int p = q + j;
-        if (p < pbeg || p >= pend) continue;
-        const uint32_t wrd = pick4(cw, j);
+        if (p < pbeg || p >= pend) {
+          rot4(cw, cw[0]);
+          rot4(px, px[0]);
+          rot4(py, py[0]);
+          rot4(pux, pux[0]);
+          rot4(puy, puy[0]);
+          rot4(puz, puz[0]);
+          continue;
+        }
+        const uint32_t wrd = cw[0];
         const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
         const int cid = (ix << 16) | iy;
         if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
@@ -567,12 +601,11 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           cache_cell = cid;
         }
         Pushed<T> o;
-        push_one<T, MIXED>(a, sp, ix, iy, pick4(px, j), pick4(py, j), pick4(pux, j), pick4(puy, j),
-                           pick4(puz, j), n00, n01, n10, n11, o);
+        push_one<T, MIXED>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
         status |= o.status;
         const bool inwin = ix == ixt && iy >= y0 && iy < y1;
         const bool cross = o.dcx != 0 || o.dcy != 0;
-        if (HIST) {
+        if (HIST && cross && inwin) {
           // new cell in the tile's window: column 1 + dcx, row new_iy - y0 + 1
           // (wrapped rows come back through +-my; a reflected particle keeps its row)
           int by = cw_iy(o.cw) - y0 + 1;
@@ -586,18 +619,34 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
               b = window_bin(ix, iy, ixt, y0, y1, TY, a.mx, a.my, a.ybc);
             }
           }
-          put4(bins, j, b);
+          const int bo = (TY + 2) + iy - y0 + 1;  // the old cell's bin
+          if (b != bo) {
+            atomicAdd(&hist[b], 1);
+            atomicAdd(&hist[bo], -1);
+          }
         }
         if (inwin) {
           const int key = iy - y0;
           if (key != acc_key) {
-            if (acc_key >= 0) {  // rare: the thread's particles changed cell
+            if (acc_key >= 0) {  // the thread's particles changed cell
+              if constexpr (MIXED) {
+                if (first_key < 0) {  // first change of the pass: keep the part for the run sums
+                  first_key = acc_key;
 #pragma unroll
-              for (int k = 0; k < 17; ++k) {
-                mycol[k * 33] = acc[k];
-                acc[k] = T(0);
+                  for (int k = 0; k < 17; ++k) {
+                    sm.first[w][k][lane] = acc[k];
+                    acc[k] = T(0);
+                  }
+                }
               }
-              flush_column<T, MIXED>(win, mycol, acc_key, WR);
+              if (acc_key >= 0 && acc_key != first_key) {  // a cell wholly inside this thread's pass
+#pragma unroll
+                for (int k = 0; k < 17; ++k) {
+                  mycol[k * 33] = acc[k];
+                  acc[k] = T(0);
+                }
+                flush_column<T, MIXED>(win, mycol, acc_key, WR);
+              }
             }
             acc_key = key;
           }
@@ -662,12 +711,12 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           for (int k = 0; k < 16; ++k) mycol[k * 33] = o.e[k];
           deposit_global<T, MIXED>(a, mycol, ix, iy, o.dcx, o.dcy, o.di, o.dj);
         }
-        put4(cw, j, o.cw);
-        put4(px, j, o.dx);
-        put4(py, j, o.dy);
-        put4(pux, j, o.ux);
-        put4(puy, j, o.uy);
-        put4(puz, j, o.uz);
+        rot4(cw, o.cw);
+        rot4(px, o.dx);
+        rot4(py, o.dy);
+        rot4(pux, o.ux);
+        rot4(puy, o.uy);
+        rot4(puz, o.uz);
         if (sp) pke_e += o.ke;
         else pke_i += o.ke;
       }
@@ -692,18 +741,6 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           }
         }
       }
-      if (HIST) {  // warp-aggregated count of the new cells
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int b0 = __shfl_sync(FULL, bins[j], 0);
-          if (__all_sync(FULL, bins[j] == b0)) {  // common: the whole warp lands in one cell
-            if (lane == 0 && b0 >= 0) atomicAdd(&hist[b0], 32);
-          } else {
-            const unsigned peers = __match_any_sync(FULL, bins[j]);
-            if (bins[j] >= 0 && (peers & lanemask_lt()) == 0) atomicAdd(&hist[bins[j]], __popc(peers));
-          }
-        }
-      }
     }
     ke_e += (double)pke_e;
     ke_i += (double)pke_i;
@@ -711,24 +748,64 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     const int key = acc_key >= 0 ? acc_key : -1 - (int)lane;
     const int kprev = __shfl_up_sync(FULL, key, 1);
     const unsigned head = (lane == 0) || (kprev != key);
-    warp_segmented_scan<T, 17>(acc, head);
-    const unsigned head_next = __shfl_down_sync(FULL, head, 1);
-    const bool tail = acc_key >= 0 && (lane == 31 || head_next);
-    __syncwarp();
+    if constexpr (MIXED) {
+      // Keys do not decrease across the lanes, so a run is the lanes head..tail
+      // plus, when the next lane's first part has the run's cell, that part. The
+      // 17 lanes sum the run's staged columns in lane order (a fixed order: the
+      // result does not depend on timing). A first part that does not continue
+      // the run ending at the previous lane is added on its own.
+      const int fnext = __shfl_down_sync(FULL, first_key, 1);
+      const unsigned heads = __ballot_sync(FULL, head);
+      const unsigned head_next = __shfl_down_sync(FULL, head, 1);
+      unsigned tails = __ballot_sync(FULL, acc_key >= 0 && (lane == 31 || head_next));
+      const bool joined = lane > 0 && head && kprev == first_key;
+      unsigned solo = __ballot_sync(FULL, first_key >= 0 && !joined);
 #pragma unroll
-    for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
-    __syncwarp();
-    unsigned tails = __ballot_sync(FULL, tail);
-    while (tails) {
-      const int src = __ffs(tails) - 1;
-      tails &= tails - 1;
-      const int kt = __shfl_sync(FULL, key, src);
-      if (lane < 17) {
-        const T v = sm.stage[w][lane][src];
-        if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+      for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
+      __syncwarp();
+      while (tails) {
+        const int src = __ffs(tails) - 1;
+        tails &= tails - 1;
+        const int start = 31 - __clz(heads & (0xffffffffu >> (31 - src)));
+        const int kt = __shfl_sync(FULL, key, src);
+        const int nf = __shfl_sync(FULL, fnext, src);
+        if (lane < 17) {
+          const T* row = &sm.stage[w][lane][0];
+          T v = row[start];
+          for (int l = start + 1; l <= src; ++l) v = __fadd_rn(v, row[l]);
+          if (src < 31 && nf == kt) v = __fadd_rn(v, sm.first[w][lane][src + 1]);
+          if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+        }
+      }
+      while (solo) {
+        const int src = __ffs(solo) - 1;
+        solo &= solo - 1;
+        const int kt = __shfl_sync(FULL, first_key, src);
+        if (lane < 17) {
+          const T v = sm.first[w][lane][src];
+          if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+        }
+      }
+    } else {
+      // plain form: segmented scan across the lanes; each run's tail holds its sum
+      warp_segmented_scan<T, 17>(acc, head);
+      const unsigned head_next = __shfl_down_sync(FULL, head, 1);
+      const bool tail = acc_key >= 0 && (lane == 31 || head_next);
+#pragma unroll
+      for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
+      __syncwarp();
+      unsigned tails = __ballot_sync(FULL, tail);
+      while (tails) {
+        const int src = __ffs(tails) - 1;
+        tails &= tails - 1;
+        const int kt = __shfl_sync(FULL, key, src);
+        if (lane < 17) {
+          const T v = sm.stage[w][lane][src];
+          if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+        }
       }
     }
-    __syncwarp();
+    __syncwarp();  // the stage is rewritten in the next pass
   }
   __syncthreads();
   // Fold the window into the global current.
@@ -760,7 +837,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 template <class T, bool MIXED, bool HIST>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ PushSmem<T> sm;
+  __shared__ PushSmem<T, MIXED> sm;
   push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES>(a, blockIdx.x, sm, smem_raw);
 }
 
@@ -770,7 +847,7 @@ template <class T, bool MIXED, bool HIST, int G>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
     k_push_batched(const PushParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ PushSmem<T> sm;
+  __shared__ PushSmem<T, MIXED> sm;
   __shared__ PushParams<T> a;
   __shared__ int next;
   while (true) {

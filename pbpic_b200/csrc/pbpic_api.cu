@@ -270,6 +270,7 @@ PushParams<T> push_params(pbpic_handle* h) {
   p.ng = (const T*)h->ng;
   p.jacc = h->jacc;
   p.tilecnt = h->tilecnt;
+  p.cell_off = h->off;
   const T dt = (T)c.dt, mime = (T)c.mime, cva = (T)c.cva, dx = (T)c.dx, dy = (T)c.dy;
   for (int s = 0; s < 2; ++s) {
     const T q = s == 0 ? T(1) : T(-1);
@@ -432,6 +433,7 @@ int do_push(pbpic_handle* h) {
   PushParams<T> p = push_params<T, MIXED>(h);
   const size_t smem = push_smem_bytes(h->TY, MIXED);
   const bool hist = h->sorted && h->fused_ok;
+  if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
   const int nt = PushThreads<T>::value;
   if (hist) k_push<T, MIXED, true><<<h->ntiles, nt, smem, s>>>(p);
   else k_push<T, MIXED, false><<<h->ntiles, nt, smem, s>>>(p);
@@ -1521,6 +1523,7 @@ int batch_descriptors(pbpic_batch* b) {
     for (int par = 0; par < 2; ++par) {
       h->cur = par == 0 ? cur0 : 1 - cur0;
       b->h_push[par * D + d] = push_params<float, true>(h);
+      if (!b->h_push[par * D + d].cell_off) return fail(PBPIC_EINVAL, "batched push: no cell offsets");
       const int i = h->cur, o = 1 - i;
       ScatterParams<float>& sp = b->h_scat[par * D + d];
       sp.mx = h->cfg.mx;
