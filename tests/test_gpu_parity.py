@@ -286,7 +286,8 @@ def test_fused_sort_is_the_stable_sort(gpu_lib, oracle_mod, precision, ybc, mx, 
     within a cell) of the pushed particles, and the per-cell counts."""
     cfg, ld, p, _ = plasma(oracle_mod, ybc, mx=mx, my=my, ppc=6, vthe=0.6)
     yee = random_fields(cfg, 5, amp=0.2)
-    with new_sim(cfg, len(p), precision=precision, tile_rows=ty) as s:
+    # the push leaves its output in pushed order; countingsort runs the fused sort
+    with new_sim(cfg, len(p), precision=precision, tile_rows=ty, options=pbpic_b200.OPT_NO_AUTOSORT) as s:
         s.load_particles(p)
         s.load_fields(yee)
         s.countingsort()
