@@ -21,18 +21,11 @@ namespace pbd {
 // --------------------------------------------------------------- scan
 constexpr int SCAN_BT = 256, SCAN_IPT = 16, SCAN_TILE = SCAN_BT * SCAN_IPT;
 
-// Exclusive scan of each SCAN_TILE chunk in place; chunk totals to sums[].
-static __global__ void __launch_bounds__(SCAN_BT) k_scan_local(int32_t* data, int64_t n, int32_t* sums) {
-  __shared__ int32_t buf[SCAN_TILE];
-  __shared__ int32_t ws[SCAN_BT / 32];
+// In-place exclusive scan of buf[0, SCAN_TILE) by a block of SCAN_BT threads
+// (the values stored, a barrier passed); ws holds SCAN_BT/32 + 1 ints. Returns
+// the chunk's total to every thread.
+__device__ __forceinline__ int32_t block_scan_excl(int32_t* buf, int32_t* ws) {
   const int t = threadIdx.x;
-  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
-#pragma unroll
-  for (int k = 0; k < SCAN_IPT; ++k) {
-    const int64_t i = base + k * SCAN_BT + t;
-    buf[k * SCAN_BT + t] = i < n ? data[i] : 0;
-  }
-  __syncthreads();
   int32_t local = 0;
 #pragma unroll
   for (int k = 0; k < SCAN_IPT; ++k) {
@@ -59,17 +52,36 @@ static __global__ void __launch_bounds__(SCAN_BT) k_scan_local(int32_t* data, in
       if (lane >= (unsigned)d) wi += y;
     }
     if (t < SCAN_BT / 32) ws[t] = wi - w;
+    if (t == SCAN_BT / 32 - 1) ws[SCAN_BT / 32] = wi;
   }
   __syncthreads();
   const int32_t excl = ws[t >> 5] + inc - local;
 #pragma unroll
   for (int k = 0; k < SCAN_IPT; ++k) buf[t * SCAN_IPT + k] += excl;
-  if (t == SCAN_BT - 1) sums[blockIdx.x] = excl + local;
   __syncthreads();
+  return ws[SCAN_BT / 32];
+}
+
+// Exclusive scan of each SCAN_TILE chunk of in[] into out[] (in may equal
+// out); chunk totals to sums[].
+static __global__ void __launch_bounds__(SCAN_BT) k_scan_local(const int32_t* in, int32_t* out, int64_t n,
+                                                              int32_t* sums) {
+  __shared__ int32_t buf[SCAN_TILE];
+  __shared__ int32_t ws[SCAN_BT / 32 + 1];
+  const int t = threadIdx.x;
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
 #pragma unroll
   for (int k = 0; k < SCAN_IPT; ++k) {
     const int64_t i = base + k * SCAN_BT + t;
-    if (i < n) data[i] = buf[k * SCAN_BT + t];
+    buf[k * SCAN_BT + t] = i < n ? in[i] : 0;
+  }
+  __syncthreads();
+  const int32_t total = block_scan_excl(buf, ws);
+  if (t == 0) sums[blockIdx.x] = total;
+#pragma unroll
+  for (int k = 0; k < SCAN_IPT; ++k) {
+    const int64_t i = base + k * SCAN_BT + t;
+    if (i < n) out[i] = buf[k * SCAN_BT + t];
   }
 }
 
@@ -315,7 +327,7 @@ struct FusedSortParams {
   int mx, my, ybc, ty, tpc, ntiles, nb;
   const int32_t* tilecnt;  // [ntiles][nb] from the push
   int32_t* counts;         // [mx*my + 1] per-cell counts (last entry 0)
-  const int32_t* off;      // exclusive scan of counts
+  int32_t* off;            // exclusive scan of counts
   int32_t* base;           // [ntiles][nb] first slot of each (tile, bin)
 };
 
@@ -337,8 +349,6 @@ __device__ __forceinline__ void fused_counts_body(const FusedSortParams& a) {
     a.counts[c] = s;
   }
 }
-
-static __global__ void k_fused_counts(FusedSortParams a) { fused_counts_body(a); }
 
 __device__ __forceinline__ void fused_base_body(const FusedSortParams& a) {
   const int64_t n = (int64_t)a.ntiles * a.nb;
@@ -366,7 +376,34 @@ __device__ __forceinline__ void fused_base_body(const FusedSortParams& a) {
   }
 }
 
-static __global__ void k_fused_base(FusedSortParams a) { fused_base_body(a); }
+static __global__ void k_fused_counts(FusedSortParams a) { fused_counts_body(a); }
+
+// After the chunk scan of the counts (k_scan_local) and the scan of the chunk
+// totals, one thread per cell: the cell's offset (its chunk's prefix added)
+// and the first slot of each (tile, bin) that holds the cell (the offset plus
+// the cell's particles in earlier tiles, as fused_base_body).
+static __global__ void k_fused_offsets(FusedSortParams a, const int32_t* sums) {
+  const int64_t ncells = (int64_t)a.mx * a.my;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t o = a.off[c] + sums[c / SCAN_TILE];
+    a.off[c] = o;
+    if (c == ncells) continue;
+    const int cx = (int)(c / a.my), cy = (int)(c - (int64_t)cx * a.my);
+    int tl[9], bl[9], cl[9];
+    const int nt = tiles_of_cell(cx, cy, a.mx, a.my, a.ybc, a.ty, a.tpc, tl);
+    for (int k = 0; k < nt; ++k) {
+      bl[k] = bin_in_tile(cx, cy, tl[k], a.mx, a.my, a.ybc, a.ty, a.tpc);
+      cl[k] = bl[k] >= 0 ? a.tilecnt[(int64_t)tl[k] * a.nb + bl[k]] : 0;
+    }
+    for (int k = 0; k < nt; ++k) {
+      if (bl[k] < 0) continue;
+      int32_t before = o;
+      for (int j = 0; j < nt; ++j)
+        if (tl[j] < tl[k]) before += cl[j];
+      a.base[(int64_t)tl[k] * a.nb + bl[k]] = before;
+    }
+  }
+}
 
 static __global__ void k_fused_counts_batched(const FusedSortParams* d) {
   __shared__ FusedSortParams a;

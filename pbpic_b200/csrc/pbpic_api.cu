@@ -81,7 +81,7 @@ int64_t scan_scratch_ints(int64_t n) {
 int scan_excl(cudaStream_t s, int32_t* data, int64_t n, int32_t* scratch) {
   if (n <= 0) return PBPIC_OK;
   int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
-  k_scan_local<<<(unsigned)nb, SCAN_BT, 0, s>>>(data, n, scratch);
+  k_scan_local<<<(unsigned)nb, SCAN_BT, 0, s>>>(data, data, n, scratch);
   CKLAUNCH("k_scan_local");
   if (nb > 1) {
     TRY(scan_excl(s, scratch, nb, scratch + nb + 1));
@@ -477,12 +477,17 @@ int do_fused_sort(pbpic_handle* h) {
   f.counts = h->counts;
   f.off = h->off;
   f.base = h->tbase;
+  // cell counts; their chunk scan into the offsets; the scan of the chunk
+  // totals; one pass per cell adding the chunk prefixes and writing the
+  // (tile, bin) first slots
   k_fused_counts<<<grid_for((int64_t)h->ncells + 1, 256), 256, 0, s>>>(f);
   CKLAUNCH("k_fused_counts");
-  CK(cudaMemcpyAsync(h->off, h->counts, (size_t)(h->ncells + 1) * 4, cudaMemcpyDeviceToDevice, s));
-  TRY(scan_excl(s, h->off, h->ncells + 1, h->scan_scratch));
-  k_fused_base<<<grid_for((int64_t)h->ntiles * h->nb, 256), 256, 0, s>>>(f);
-  CKLAUNCH("k_fused_base");
+  const int64_t nchunks = ((int64_t)h->ncells + 1 + SCAN_TILE - 1) / SCAN_TILE;
+  k_scan_local<<<(unsigned)nchunks, SCAN_BT, 0, s>>>(h->counts, h->off, (int64_t)h->ncells + 1, h->scan_scratch);
+  CKLAUNCH("k_scan_local");
+  TRY(scan_excl(s, h->scan_scratch, nchunks, h->scan_scratch + nchunks + 1));
+  k_fused_offsets<<<grid_for((int64_t)h->ncells + 1, 256), 256, 0, s>>>(f, h->scan_scratch);
+  CKLAUNCH("k_fused_offsets");
   const int b = h->cur, o = 1 - b;
   ScatterParams<T> sp;
   sp.mx = f.mx;
