@@ -353,7 +353,7 @@ def main():
                    "l2": "inputs larger than L2 (particle state 2.5 GB)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved_push, "peak": peak, "unit": "GB/s",
                      "frac": achieved_push / peak, "traffic": PUSH_DRAM_BYTES_PER_PARTICLE * n,
-                     "kernel": "k_push<float,true,true>",
+                     "kernel": "k_push<float,true,true,false>",
                      "bytes_per_launch": bytes_push, "peak_kind": peak_kind,
                      "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak},
         "phase_ms": {"push": m["t_push"], "fieldsolve": m["t_field"], "sort": m["t_sort"]},

@@ -128,7 +128,9 @@ struct Pushed {
 
 // Push of one particle whose gather nodes are n00 (ix,iy), n01 (ix,iy+1),
 // n10 (ix+1,iy), n11 (ix+1,iy+1). MIXED is only instantiated with T = float.
-template <class T, bool MIXED>
+// COMPAT = false compiles the step for a configuration without the compat
+// switches of the push (the rho weights are then the gather weights).
+template <class T, bool MIXED, bool COMPAT = true>
 __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux,
                                          T puy, T puz, const Node6<T>& n00, const Node6<T>& n01,
                                          const Node6<T>& n10, const Node6<T>& n11, Pushed<T>& o) {
@@ -163,7 +165,7 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
     t2 = A::div(T(2), tsq1);
   }
   const T sx = A::mul(t2, tx), sy = A::mul(t2, ty), sz = A::mul(t2, tz);
-  const bool cb = (a.compat & 1) != 0;  // rotate the pre-kick momentum (pic2d.f90:985-987)
+  const bool cb = COMPAT && (a.compat & 1) != 0;  // rotate the pre-kick momentum (pic2d.f90:985-987)
   const T vx = cb ? pux : umx, vy = cb ? puy : umy, vz0 = cb ? puz : umz;
   const T u0x = A::add(umx, A::mad(vy, tz, -A::mul(vz0, ty)));
   const T u0y = A::add(umy, A::mad(vz0, tx, -A::mul(vx, tz)));
@@ -277,7 +279,7 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
     o.e[11] = A::mul(quz, z1);  // jz (di, dj)
   }
   {
-    const bool cr = (a.compat & 4) != 0;  // mirrored weights (pic2d.f90:1285-1288)
+    const bool cr = COMPAT && (a.compat & 4) != 0;  // mirrored weights (pic2d.f90:1285-1288)
     const T rx = cr ? A::sub(half, px) : A::add(half, px);
     const T ry = cr ? A::sub(half, py) : A::add(half, py);
     const T r1 = A::mul(rx, ry);
@@ -492,7 +494,7 @@ __device__ __forceinline__ void rot4(V (&v)[4], V x) {
 // Push of tile t of the domain `a`, by all threads of the block. G float4
 // groups of particles per thread per pass (8 particles for G = 2).
 // smem_raw: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
-template <class T, bool MIXED, bool HIST, int G>
+template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true>
 __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
                                           unsigned char* smem_raw) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
@@ -601,7 +603,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           cache_cell = cid;
         }
         Pushed<T> o;
-        push_one<T, MIXED>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
+        push_one<T, MIXED, COMPAT>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
         status |= o.status;
         const bool inwin = ix == ixt && iy >= y0 && iy < y1;
         const bool cross = o.dcx != 0 || o.dcy != 0;
@@ -833,17 +835,17 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   if (lane == 0 && status) atomicOr(a.status, status);
 }
 
-// Single domain: one block per tile.
-template <class T, bool MIXED, bool HIST>
+// Single domain: one block per tile. COMPAT = false when no compat switch is set.
+template <class T, bool MIXED, bool HIST, bool COMPAT>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T, MIXED> sm;
-  push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES>(a, blockIdx.x, sm, smem_raw);
+  push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES, COMPAT>(a, blockIdx.x, sm, smem_raw);
 }
 
 // Batched domains: persistent blocks take (domain, tile) pairs from a global
 // counter (reset to 0 before each launch) in the order of `tiles`.
-template <class T, bool MIXED, bool HIST, int G>
+template <class T, bool MIXED, bool HIST, int G, bool COMPAT>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
     k_push_batched(const PushParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -858,7 +860,7 @@ __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINB
     const int2 it = tiles[t];
     if (threadIdx.x == 0) a = descs[it.x];
     __syncthreads();
-    push_tile<T, MIXED, HIST, G>(a, it.y, sm, smem_raw);
+    push_tile<T, MIXED, HIST, G, COMPAT>(a, it.y, sm, smem_raw);
     __syncthreads();
   }
 }

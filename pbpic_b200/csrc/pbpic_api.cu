@@ -435,8 +435,11 @@ int do_push(pbpic_handle* h) {
   const bool hist = h->sorted && h->fused_ok;
   if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
   const int nt = PushThreads<T>::value;
-  if (hist) k_push<T, MIXED, true><<<h->ntiles, nt, smem, s>>>(p);
-  else k_push<T, MIXED, false><<<h->ntiles, nt, smem, s>>>(p);
+  const bool compat = h->cfg.compat != 0;
+  if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
+  else if (hist) k_push<T, MIXED, true, true><<<h->ntiles, nt, smem, s>>>(p);
+  else if (!compat) k_push<T, MIXED, false, false><<<h->ntiles, nt, smem, s>>>(p);
+  else k_push<T, MIXED, false, true><<<h->ntiles, nt, smem, s>>>(p);
   CKLAUNCH("k_push");
   k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
   CKLAUNCH("k_energy_row");
@@ -1353,6 +1356,7 @@ struct pbpic_batch {
   std::vector<pbpic_handle*> dom;
   cudaStream_t stream = nullptr;
   int groups = PBPIC_PUSH_HALVES;  // particles per thread / 4 in the push
+  bool compat = true;              // some domain sets a compat switch (generic push)
   int64_t launches_per_pair = 0;
   cudaGraphExec_t graph = nullptr;
   // descriptor tables: host copies (kept alive for the asynchronous uploads) and device arrays
@@ -1494,11 +1498,13 @@ int batch_layout(pbpic_batch* b) {
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   int per_sm = 1;
-  if (b->groups == 1) {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 1>, PushThreads<float>::value, smem));
-  } else {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_batched<float, true, true, 2>, PushThreads<float>::value, smem));
-  }
+  b->compat = false;
+  for (pbpic_handle* h : b->dom) b->compat |= h->cfg.compat != 0;
+  const void* fn = b->groups == 1 ? (b->compat ? (const void*)k_push_batched<float, true, true, 1, true>
+                                               : (const void*)k_push_batched<float, true, true, 1, false>)
+                                  : (b->compat ? (const void*)k_push_batched<float, true, true, 2, true>
+                                               : (const void*)k_push_batched<float, true, true, 2, false>);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PushThreads<float>::value, smem));
   b->push_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_scatter_batched<float>, 256, 0));
   b->scatter_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
@@ -1610,10 +1616,15 @@ int batch_enqueue_step(pbpic_batch* b, int par) {
   k_batch_begin<<<dim3(b->gx_zero, D), 256, 0, s>>>(b->d_dom, ctr, ctr + 2);
   CKLAUNCH("k_batch_begin");
   const PushParams<float>* pp = b->d_push + (size_t)par * D;
-  if (b->groups == 1)
-    k_push_batched<float, true, true, 1><<<b->push_blocks, PushThreads<float>::value, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+  const unsigned nt = PushThreads<float>::value;
+  if (b->groups == 1 && b->compat)
+    k_push_batched<float, true, true, 1, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+  else if (b->groups == 1)
+    k_push_batched<float, true, true, 1, false><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+  else if (b->compat)
+    k_push_batched<float, true, true, 2, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   else
-    k_push_batched<float, true, true, 2><<<b->push_blocks, PushThreads<float>::value, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 2, false><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   CKLAUNCH("k_push_batched");
   k_fused_counts_batched<<<dim3(b->gx_cells, D), 256, 0, s>>>(b->d_fsort);
   CKLAUNCH("k_fused_counts_batched");
