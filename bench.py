@@ -29,9 +29,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy error"
-# DRAM bytes per particle of one k_push launch (read + write) from the ncu capture summarised in
-# profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to the particles.
-PUSH_DRAM_BYTES_PER_PARTICLE = 48.6
+# DRAM bytes per particle of one k_push launch (read + write: the state read through the sort's
+# permutation, the permutation itself, the state written in cell order) from the ncu capture
+# summarised in profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to
+# the particles.
+PUSH_DRAM_BYTES_PER_PARTICLE = 60.4
 UNIT = "particle-steps/s"
 
 
@@ -353,7 +355,7 @@ def main():
                    "l2": "inputs larger than L2 (particle state 2.5 GB)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved_push, "peak": peak, "unit": "GB/s",
                      "frac": achieved_push / peak, "traffic": PUSH_DRAM_BYTES_PER_PARTICLE * n,
-                     "kernel": "k_push<float,true,true,false>",
+                     "kernel": "k_push<float,true,true,false,true>",
                      "bytes_per_launch": bytes_push, "peak_kind": peak_kind,
                      "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak},
         "phase_ms": {"push": m["t_push"], "fieldsolve": m["t_field"], "sort": m["t_sort"]},

@@ -36,6 +36,11 @@
 // not depend on the order of the atomics, so the result is the same bits
 // either way.
 //
+// With GATHER the input is the previous step's arrays in their own order and
+// the fused sort's permutation (sorted position -> element): the push reads
+// each particle through it and writes the result in sorted position to a
+// second set of arrays, so that the sort never moves the particle data.
+//
 // With HIST the kernel also counts the new cells of its particles in the
 // tile's window (the 3x3 neighbourhood of the tile), the first half of the
 // fused counting sort (kernels_sort.cuh). The input is sorted, so the counts
@@ -58,6 +63,13 @@ struct PushParams {
   void* jacc;       // 4 planes (jx, jy, jz, rho) of mx x S accumulators
   int32_t* tilecnt; // [ntiles][3*(tile_rows+2)] new-cell counts (HIST)
   const int32_t* cell_off;  // [mx*my + 1] cell offsets of the sorted input (HIST)
+  // GATHER: particle p of the sorted order is element src[p] of the input
+  // arrays above; its result goes to element p of the output arrays.
+  const int32_t* src;
+  uint32_t* cell_o;
+  T *dx_o, *dy_o, *ux_o, *uy_o, *uz_o;
+  const int32_t* pid_i;  // tracked ids, moved with the particles (null: none)
+  int32_t* pid_o;
   T c0[2], c1[2], ms[2], qx[2], qy[2], q[2];  // per species: 0 ion, 1 electron
   T dtcva, idx, idy, cva;
   double* ke_part;  // [ntiles][2]: electron, ion kinetic energy of the tile
@@ -494,7 +506,7 @@ __device__ __forceinline__ void rot4(V (&v)[4], V x) {
 // Push of tile t of the domain `a`, by all threads of the block. G float4
 // groups of particles per thread per pass (8 particles for G = 2).
 // smem_raw: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
-template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true>
+template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true, bool GATHER = false>
 __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
                                           unsigned char* smem_raw) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
@@ -554,7 +566,30 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
       uint32_t cw[4];
       T px[4], py[4], pux[4], puy[4], puz[4];
       const bool full = q >= pbeg && q + 4 <= pend;
-      if (full) {
+      int32_t sidx[4] = {0, 0, 0, 0};  // GATHER: input elements of the group
+      if (GATHER) {
+        if (full) {
+          ld4(reinterpret_cast<const uint32_t*>(a.src) + q, reinterpret_cast<uint32_t(&)[4]>(sidx));
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int p = q + j;
+            sidx[j] = (p >= pbeg && p < pend) ? a.src[p] : 0;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int p = q + j;
+          const bool act = p >= pbeg && p < pend;
+          const int e = sidx[j];
+          cw[j] = act ? a.cell[e] : 0u;
+          px[j] = act ? a.dx[e] : T(0);
+          py[j] = act ? a.dy[e] : T(0);
+          pux[j] = act ? a.ux[e] : T(0);
+          puy[j] = act ? a.uy[e] : T(0);
+          puz[j] = act ? a.uz[e] : T(0);
+        }
+      } else if (full) {
         ld4(a.cell + q, cw);
         ld4(a.dx + q, px);
         ld4(a.dy + q, py);
@@ -722,25 +757,35 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         if (sp) pke_e += o.ke;
         else pke_i += o.ke;
       }
+      uint32_t* ocell = GATHER ? a.cell_o : a.cell;
+      T *odx = GATHER ? a.dx_o : a.dx, *ody = GATHER ? a.dy_o : a.dy;
+      T *oux = GATHER ? a.ux_o : a.ux, *ouy = GATHER ? a.uy_o : a.uy, *ouz = GATHER ? a.uz_o : a.uz;
       if (full) {
-        st4(a.cell + q, cw);
-        st4(a.dx + q, px);
-        st4(a.dy + q, py);
-        st4(a.ux + q, pux);
-        st4(a.uy + q, puy);
-        st4(a.uz + q, puz);
+        st4(ocell + q, cw);
+        st4(odx + q, px);
+        st4(ody + q, py);
+        st4(oux + q, pux);
+        st4(ouy + q, puy);
+        st4(ouz + q, puz);
       } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int p = q + j;
           if (p >= pbeg && p < pend) {
-            a.cell[p] = cw[j];
-            a.dx[p] = px[j];
-            a.dy[p] = py[j];
-            a.ux[p] = pux[j];
-            a.uy[p] = puy[j];
-            a.uz[p] = puz[j];
+            ocell[p] = cw[j];
+            odx[p] = px[j];
+            ody[p] = py[j];
+            oux[p] = pux[j];
+            ouy[p] = puy[j];
+            ouz[p] = puz[j];
           }
+        }
+      }
+      if (GATHER && a.pid_o) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int p = q + j;
+          if (p >= pbeg && p < pend) a.pid_o[p] = a.pid_i[sidx[j]];
         }
       }
     }
@@ -835,12 +880,14 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   if (lane == 0 && status) atomicOr(a.status, status);
 }
 
-// Single domain: one block per tile. COMPAT = false when no compat switch is set.
-template <class T, bool MIXED, bool HIST, bool COMPAT>
+// Single domain: one block per tile. COMPAT = false when no compat switch is
+// set; GATHER when the input is the previous step's arrays and the sort's
+// permutation.
+template <class T, bool MIXED, bool HIST, bool COMPAT, bool GATHER = false>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T, MIXED> sm;
-  push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES, COMPAT>(a, blockIdx.x, sm, smem_raw);
+  push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES, COMPAT, GATHER>(a, blockIdx.x, sm, smem_raw);
 }
 
 // Batched domains: persistent blocks take (domain, tile) pairs from a global

@@ -524,175 +524,43 @@ __device__ __forceinline__ void scatter_tile(const ScatterParams<T>& a, const in
   }
 }
 
+// ------------------------------------------------- permutation-only sort
+// The same stable ranking as scatter_tile, reading only the cell words: the
+// particle at array element p of the tile gets its sorted slot d, and
+// perm[d] = p. The particle data stay where they are; the next push reads
+// them through perm (PushParams::src), and a gather (k_gather) applies perm
+// when the arrays themselves must be in cell order.
+constexpr int SP_IPT = 8, SP_CHUNK = 256 * SP_IPT;
+
 template <class T>
-__global__ void __launch_bounds__(256) k_fused_scatter(ScatterParams<T> a) {
+__global__ void __launch_bounds__(256) k_fused_perm(ScatterParams<T> a, int32_t* perm) {
   __shared__ ScatterSmem sm;
-  scatter_tile(a, blockIdx.x, sm);
-}
-
-// ------------------------------------------- scatter with bulk-copy staging
-// The same stable scatter, with each chunk's particle arrays brought into
-// shared memory by the bulk-copy (TMA) engine, cp.async.bulk, in a ring of
-// SB_NS buffers: while the block ranks and writes chunk k, the copies of
-// chunks k+1 .. k+SB_NS-1 are in flight, so the DRAM stream does not wait on
-// the ranking. Copies
-// start on 16-byte boundaries (the chunk start rounded down, its end rounded
-// up; particle arrays carry 16 elements of padding) and complete on an
-// mbarrier. Every wait is bounded (2 s of %globaltimer): on a timeout the
-// block sets status bit 16, waits (bounded again) for its copies still in
-// flight and returns.
-#ifndef PBPIC_SCATTER_STAGES
-#define PBPIC_SCATTER_STAGES 3
-#endif
-constexpr int SB_IPT = 4, SB_CH = 256 * SB_IPT, SB_NS = PBPIC_SCATTER_STAGES;
-
-template <class T>
-struct StageLayout {
-  static constexpr int P4 = 4;                     // 16 bytes of 4-byte elements
-  static constexpr int PT = 16 / (int)sizeof(T);   // 16 bytes of T
-  static constexpr int N4 = SB_CH + 2 * P4;        // capacity of a 4-byte array buffer
-  static constexpr int NT = SB_CH + 2 * PT;
-  static constexpr size_t BUF = (size_t)2 * N4 * 4 + (size_t)5 * NT * sizeof(T);  // cell, pid, 5 x T
-  static constexpr size_t BYTES = SB_NS * BUF;     // ring of SB_NS buffers
-};
-
-struct StageSmem {
-  int32_t cnt[8][SC_MAXNB];
-  int32_t run[SC_MAXNB], sbase[SC_MAXNB];
-  unsigned long long bar[SB_NS];
-  int ok;
-};
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(done)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Bounded wait for the phase with `parity` of `bar` (2 s); false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  const unsigned long long t0 = globaltimer_ns();
-  while (!mbar_try_wait(bar, parity)) {
-    if (globaltimer_ns() - t0 > 2000000000ull) return false;
-  }
-  return true;
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
-template <class T>
-struct StageView {
-  uint32_t* cell;
-  int32_t* pid;
-  T* v[5];
-};
-
-template <class T>
-__device__ __forceinline__ StageView<T> stage_view(unsigned char* base, int buf) {
-  using L = StageLayout<T>;
-  unsigned char* b = base + (size_t)buf * L::BUF;
-  StageView<T> s;
-  s.cell = reinterpret_cast<uint32_t*>(b);
-  s.pid = reinterpret_cast<int32_t*>(b + (size_t)L::N4 * 4);
-#pragma unroll
-  for (int k = 0; k < 5; ++k)
-    s.v[k] = reinterpret_cast<T*>(b + (size_t)2 * L::N4 * 4 + (size_t)k * L::NT * sizeof(T));
-  return s;
-}
-
-// Thread 0: bulk copies of particles [c0, c1) into buffer `buf`.
-template <class T>
-__device__ __forceinline__ void stage_issue(const ScatterParams<T>& a, unsigned char* base, int buf, int c0, int c1,
-                                            unsigned long long* bar) {
-  using L = StageLayout<T>;
-  const int e40 = c0 & ~(L::P4 - 1), e41 = (c1 + L::P4 - 1) & ~(L::P4 - 1);
-  const int eT0 = c0 & ~(L::PT - 1), eT1 = (c1 + L::PT - 1) & ~(L::PT - 1);
-  const unsigned b4 = (unsigned)(e41 - e40) * 4u, bT = (unsigned)(eT1 - eT0) * (unsigned)sizeof(T);
-  const unsigned total = b4 * (a.pidi ? 2u : 1u) + 5u * bT;
-  StageView<T> s = stage_view<T>(base, buf);
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the buffer was read by the threads
-  mbar_expect_tx(bar, total);
-  bulk_g2s(s.cell, a.ci + e40, b4, bar);
-  if (a.pidi) bulk_g2s(s.pid, a.pidi + e40, b4, bar);
-  const T* src[5] = {a.dxi, a.dyi, a.uxi, a.uyi, a.uzi};
-#pragma unroll
-  for (int k = 0; k < 5; ++k) bulk_g2s(s.v[k], src[k] + eT0, bT, bar);
-}
-
-template <class T>
-__device__ __forceinline__ void scatter_tile_staged(const ScatterParams<T>& a, const int t, StageSmem& sm,
-                                                    unsigned char* stage, unsigned& phase, int* status) {
-  using L = StageLayout<T>;
   int32_t(&cnt)[8][SC_MAXNB] = sm.cnt;
+  const int t = blockIdx.x;
   const int ixt = t / a.tpc, y0 = (t - ixt * a.tpc) * a.ty, y1 = min(y0 + a.ty, a.my);
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
-  const int nchunks = (pend - pbeg + SB_CH - 1) / SB_CH;
   const int w = threadIdx.x >> 5;
   const unsigned lane = lane_id(), lt = lanemask_lt();
   for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
     sm.run[b] = 0;
     sm.sbase[b] = a.base[(int64_t)t * a.nb + b];
   }
-  // `phase` holds the parity bit of each ring buffer's next completion
-  if (threadIdx.x == 0)
-    for (int k = 0; k < SB_NS && k < nchunks; ++k)
-      stage_issue(a, stage, k, pbeg + k * SB_CH, min(pbeg + (k + 1) * SB_CH, pend), &sm.bar[k]);
-  for (int k = 0; k < nchunks; ++k) {
-    const int buf = k % SB_NS;
-    const unsigned par = (phase >> buf) & 1u;
-    const int c0 = pbeg + k * SB_CH, c1 = min(c0 + SB_CH, pend);
+  for (int c0 = pbeg; c0 < pend; c0 += SP_CHUNK) {
     for (int e = threadIdx.x; e < 8 * SC_MAXNB; e += blockDim.x) (&cnt[0][0])[e] = 0;
-    if (threadIdx.x == 0) sm.ok = mbar_wait_bounded(&sm.bar[buf], par) ? 1 : 0;
     __syncthreads();
-    if (!sm.ok) {  // the copy did not arrive: flag, drain what is in flight, give up the tile
-      if (threadIdx.x == 0) {
-        atomicOr(status, 16);
-        for (int j = 0; j < SB_NS && k + j < nchunks; ++j) {
-          const int bj = (k + j) % SB_NS;
-          mbar_wait_bounded(&sm.bar[bj], (phase >> bj) & 1u);
-        }
-      }
-      __syncthreads();
-      return;
-    }
-    mbar_wait_bounded(&sm.bar[buf], par);  // completed: every thread acquires the copied data
-    phase ^= 1u << buf;
-    const StageView<T> s = stage_view<T>(stage, buf);
-    const int s4 = c0 - (c0 & ~(L::P4 - 1)), sT = c0 - (c0 & ~(L::PT - 1));
-    int bin[SB_IPT], pos[SB_IPT];
+    int bin[SP_IPT], pos[SP_IPT];
+    uint32_t vc[SP_IPT];
 #pragma unroll
-    for (int kk = 0; kk < SB_IPT; ++kk) {
-      const int i = w * (32 * SB_IPT) + kk * 32 + (int)lane;
+    for (int k = 0; k < SP_IPT; ++k) {  // every load of the chunk before the ranking
+      const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
+      vc[k] = p < pend ? a.ci[p] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < SP_IPT; ++k) {
+      const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
       int b = a.nb;  // sentinel: beyond the tile
-      if (c0 + i < c1) {
-        const uint32_t cw = s.cell[s4 + i];
-        b = window_bin(cw_ix(cw), cw_iy(cw), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
+      if (p < pend) {
+        b = window_bin(cw_ix(vc[k]), cw_iy(vc[k]), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
         if (b < 0) b = a.nb;  // cannot happen: the push kept every particle in its window
       }
       const unsigned peers = __match_any_sync(FULL, b);
@@ -700,8 +568,8 @@ __device__ __forceinline__ void scatter_tile_staged(const ScatterParams<T>& a, c
       __syncwarp();
       if ((peers & lt) == 0) cnt[w][b] = before + __popc(peers);
       __syncwarp();
-      pos[kk] = before + __popc(peers & lt);
-      bin[kk] = b;
+      pos[k] = before + __popc(peers & lt);
+      bin[k] = b;
     }
     __syncthreads();
     for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
@@ -716,36 +584,14 @@ __device__ __forceinline__ void scatter_tile_staged(const ScatterParams<T>& a, c
     }
     __syncthreads();
 #pragma unroll
-    for (int kk = 0; kk < SB_IPT; ++kk) {
-      if (bin[kk] < a.nb) {
-        const int i = w * (32 * SB_IPT) + kk * 32 + (int)lane;
-        const int64_t d = (int64_t)sm.sbase[bin[kk]] + cnt[w][bin[kk]] + pos[kk];
-        a.co[d] = s.cell[s4 + i];
-        a.dxo[d] = s.v[0][sT + i];
-        a.dyo[d] = s.v[1][sT + i];
-        a.uxo[d] = s.v[2][sT + i];
-        a.uyo[d] = s.v[3][sT + i];
-        a.uzo[d] = s.v[4][sT + i];
-        if (a.pido) a.pido[d] = s.pid[s4 + i];
+    for (int k = 0; k < SP_IPT; ++k) {
+      if (bin[k] < a.nb) {
+        const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
+        perm[(int64_t)sm.sbase[bin[k]] + cnt[w][bin[k]] + pos[k]] = p;
       }
     }
-    __syncthreads();  // buffer `buf` is free again
-    if (threadIdx.x == 0 && k + SB_NS < nchunks)
-      stage_issue(a, stage, buf, pbeg + (k + SB_NS) * SB_CH, min(pbeg + (k + SB_NS + 1) * SB_CH, pend), &sm.bar[buf]);
+    __syncthreads();
   }
-}
-
-template <class T>
-__global__ void __launch_bounds__(256) k_fused_scatter_staged(ScatterParams<T> a, int* status) {
-  extern __shared__ __align__(128) unsigned char stage[];
-  __shared__ StageSmem sm;
-  if (threadIdx.x == 0) {
-    for (int j = 0; j < SB_NS; ++j) mbar_init(&sm.bar[j], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  unsigned phase = 0u;
-  scatter_tile_staged(a, blockIdx.x, sm, stage, phase, status);
 }
 
 // Batched domains: persistent blocks take (domain, tile) pairs from a counter.

@@ -161,6 +161,12 @@ struct pbpic_handle {
   bool sorted = false;
   bool fused_ok = false;    // grid admits the fused counting sort (distinct window cells)
   bool hist_valid = false;  // the last push counted new cells per tile on a sorted array
+  // The fused sort leaves the particle data in place and writes perm (sorted
+  // position -> element); while `lazy`, the cell order is the arrays read
+  // through perm. The next push reads through it; every other reader of the
+  // particle arrays applies it first (materialize).
+  int32_t* perm = nullptr;
+  bool lazy = false;
   int nb = 0;               // window bins per tile, 3*(TY+2)
   int tile_cap = 0;         // tiles the per-tile arrays hold
   int64_t bin_cap = 0;      // (tile, bin) entries tilecnt and tbase hold
@@ -271,6 +277,11 @@ PushParams<T> push_params(pbpic_handle* h) {
   p.jacc = h->jacc;
   p.tilecnt = h->tilecnt;
   p.cell_off = h->off;
+  p.src = nullptr;
+  p.cell_o = nullptr;
+  p.dx_o = p.dy_o = p.ux_o = p.uy_o = p.uz_o = nullptr;
+  p.pid_i = nullptr;
+  p.pid_o = nullptr;
   const T dt = (T)c.dt, mime = (T)c.mime, cva = (T)c.cva, dx = (T)c.dx, dy = (T)c.dy;
   for (int s = 0; s < 2; ++s) {
     const T q = s == 0 ? T(1) : T(-1);
@@ -353,11 +364,35 @@ int kinetic_row(pbpic_handle* h, int row) {
   return PBPIC_OK;
 }
 
+// Apply the fused sort's permutation to the particle arrays (they are then in
+// cell order themselves); a no-op unless the handle is lazy.
+template <class T>
+int materialize_t(pbpic_handle* h) {
+  const int64_t n = h->n;
+  const int b = h->cur, o = 1 - b;
+  if (n > 0) {
+    k_gather<T><<<grid_for(n, 256), 256, 0, h->stream>>>(h->perm, n, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
+                                                          P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b],
+                                                          h->cell[o], P<T>(h, o, 0), P<T>(h, o, 1), P<T>(h, o, 2),
+                                                          P<T>(h, o, 3), P<T>(h, o, 4), h->pid[o]);
+    CKLAUNCH("k_gather");
+    h->cur = o;
+  }
+  h->lazy = false;
+  return PBPIC_OK;
+}
+
+int materialize(pbpic_handle* h) {
+  if (!h->lazy) return PBPIC_OK;
+  return h->mixed ? materialize_t<float>(h) : materialize_t<double>(h);
+}
+
 int set_unsorted_tiles(pbpic_handle* h) {
   k_tile_off_uniform<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, h->stream>>>(h->ntiles, h->n, h->tile_off);
   CKLAUNCH("k_tile_off_uniform");
   h->sorted = false;
   h->hist_valid = false;
+  h->lazy = false;
   return PBPIC_OK;
 }
 
@@ -436,30 +471,35 @@ int do_push(pbpic_handle* h) {
   if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
   const int nt = PushThreads<T>::value;
   const bool compat = h->cfg.compat != 0;
-  if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
-  else if (hist) k_push<T, MIXED, true, true><<<h->ntiles, nt, smem, s>>>(p);
-  else if (!compat) k_push<T, MIXED, false, false><<<h->ntiles, nt, smem, s>>>(p);
-  else k_push<T, MIXED, false, true><<<h->ntiles, nt, smem, s>>>(p);
-  CKLAUNCH("k_push");
+  if (h->lazy) {  // read through the sort's permutation, write in cell order to the other buffer
+    if (!hist) return fail(PBPIC_ESTATE, "k_push: a permuted input needs the sort's tables");
+    const int o = 1 - h->cur;
+    p.src = h->perm;
+    p.cell_o = h->cell[o];
+    p.dx_o = P<T>(h, o, 0);
+    p.dy_o = P<T>(h, o, 1);
+    p.ux_o = P<T>(h, o, 2);
+    p.uy_o = P<T>(h, o, 3);
+    p.uz_o = P<T>(h, o, 4);
+    p.pid_i = h->pid[h->cur];
+    p.pid_o = h->pid[o];
+    if (!compat) k_push<T, MIXED, true, false, true><<<h->ntiles, nt, smem, s>>>(p);
+    else k_push<T, MIXED, true, true, true><<<h->ntiles, nt, smem, s>>>(p);
+    CKLAUNCH("k_push");
+    h->cur = o;
+    h->lazy = false;
+  } else {
+    if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
+    else if (hist) k_push<T, MIXED, true, true><<<h->ntiles, nt, smem, s>>>(p);
+    else if (!compat) k_push<T, MIXED, false, false><<<h->ntiles, nt, smem, s>>>(p);
+    else k_push<T, MIXED, false, true><<<h->ntiles, nt, smem, s>>>(p);
+    CKLAUNCH("k_push");
+  }
   k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
   CKLAUNCH("k_energy_row");
   h->hist_valid = hist;
   h->sorted = false;
   if (autosort) TRY((do_fused_sort<T, MIXED>(h)));
-  return PBPIC_OK;
-}
-
-// The staged scatter takes more than the default 48 KB of dynamic shared
-// memory; the attribute is set once per process (one device per process).
-template <class T>
-int staged_scatter_attr() {
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
-  std::call_once(once, [] {
-    err = cudaFuncSetAttribute(k_fused_scatter_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)StageLayout<T>::BYTES);
-  });
-  if (err != cudaSuccess) return fail(PBPIC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
   return PBPIC_OK;
 }
 
@@ -491,8 +531,7 @@ int do_fused_sort(pbpic_handle* h) {
   TRY(scan_excl(s, h->scan_scratch, nchunks, h->scan_scratch + nchunks + 1));
   k_fused_offsets<<<grid_for((int64_t)h->ncells + 1, 256), 256, 0, s>>>(f, h->scan_scratch);
   CKLAUNCH("k_fused_offsets");
-  const int b = h->cur, o = 1 - b;
-  ScatterParams<T> sp;
+  ScatterParams<T> sp{};  // the ranking reads the cell words and the tables only
   sp.mx = f.mx;
   sp.my = f.my;
   sp.ybc = f.ybc;
@@ -501,25 +540,12 @@ int do_fused_sort(pbpic_handle* h) {
   sp.nb = f.nb;
   sp.tile_off = h->tile_off;
   sp.base = h->tbase;
-  sp.ci = h->cell[b];
-  sp.dxi = P<T>(h, b, 0);
-  sp.dyi = P<T>(h, b, 1);
-  sp.uxi = P<T>(h, b, 2);
-  sp.uyi = P<T>(h, b, 3);
-  sp.uzi = P<T>(h, b, 4);
-  sp.pidi = h->pid[b];
-  sp.co = h->cell[o];
-  sp.dxo = P<T>(h, o, 0);
-  sp.dyo = P<T>(h, o, 1);
-  sp.uxo = P<T>(h, o, 2);
-  sp.uyo = P<T>(h, o, 3);
-  sp.uzo = P<T>(h, o, 4);
-  sp.pido = h->pid[o];
-  if (n > 0) {
-    TRY(staged_scatter_attr<T>());
-    k_fused_scatter_staged<T><<<h->ntiles, 256, StageLayout<T>::BYTES, s>>>(sp, h->status);
-    CKLAUNCH("k_fused_scatter_staged");
-    h->cur = o;
+  sp.ci = h->cell[h->cur];
+  if (n > 0) {  // the sorted order as a permutation; the particle data stay in place
+    if (!h->perm) TRY(dalloc(h, &h->perm, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
+    k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp, h->perm);
+    CKLAUNCH("k_fused_perm");
+    h->lazy = true;
   }
   k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, h->cfg.my,
                                                                   (int32_t)n, h->tile_off);
@@ -665,6 +691,7 @@ int do_load_aos(pbpic_handle* h, const RefRec<R>* host, int64_t n) {
 
 template <class T, bool MIXED, class R>
 int do_store_aos(pbpic_handle* h, RefRec<R>* host, int64_t cap, int64_t* nout) {
+  TRY(materialize(h));
   if (nout) *nout = h->n;
   const int64_t n = std::min<int64_t>(cap, h->n);
   if (n <= 0) return PBPIC_OK;
@@ -738,6 +765,9 @@ int do_init_plasma(pbpic_handle* h, const pbpic_loader* ld) {
   }
   h->n = n;
   h->itime = 0;
+  h->sorted = false;  // new particles, in load order
+  h->hist_valid = false;
+  h->lazy = false;
   // initial fields (initfields, pic2d.f90:583-648)
   pic::FieldInit fi;
   fi.kind = ld->kind;
@@ -765,6 +795,7 @@ int do_init_plasma(pbpic_handle* h, const pbpic_loader* ld) {
 
 template <class T, bool MIXED>
 int do_gauss(pbpic_handle* h, double* out) {
+  TRY(materialize(h));
   cudaStream_t s = h->stream;
   const int64_t pe = plane_elems(h);
   CK(cudaMemsetAsync(h->rho, 0, (size_t)pe * 8, s));
@@ -1067,6 +1098,7 @@ int pbpic_energy_spectra(pbpic_handle* h, double de_electron, double de_ion, int
   if (!counts) return fail(PBPIC_EINVAL, "null buffer");
   if (!(de_electron > 0 && de_ion > 0) || nbins < 1 || nbins > 8192)
     return fail(PBPIC_EINVAL, "spectra need positive bin widths and 1..8192 bins");
+  TRY(materialize(h));
   const size_t bytes = (size_t)2 * nbins * 8;
   TRY(ensure_staging(h, bytes));
   cudaStream_t s = h->stream;
@@ -1404,6 +1436,7 @@ int batch_tile_rows(const pbpic_handle* h, int ty) {
 // recompute its tile ranges (from the cell offsets when sorted).
 int retile(pbpic_handle* h, int ty) {
   if (ty == h->TY) return PBPIC_OK;
+  TRY(materialize(h));
   const pbpic_config& c = h->cfg;
   const int tpc = (c.my + ty - 1) / ty;
   const int ntiles = c.mx * tpc;
@@ -1692,6 +1725,7 @@ int batch_step(pbpic_batch* b, int nsteps) {
   for (pbpic_handle* h : b->dom)
     if (h->filters) return fail(PBPIC_EINVAL, "the batched form does not apply field filters");
   for (pbpic_handle* h : b->dom) {
+    TRY(materialize(h));
     if (!h->sorted) TRY(do_sort<float, true>(h));
     TRY(ensure_hist(h, h->itime + nsteps + 2));
   }
@@ -2133,6 +2167,7 @@ int band_extract_sorted(pbpic_handle* h, int y_lo, int y_hi, int my_global, int 
 template <class T, bool MIXED>
 int do_band_extract(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_offset, void* dst, int64_t cap,
                     int64_t* nout) {
+  TRY(materialize(h));
   if (h->sorted) return band_extract_sorted<T, MIXED>(h, y_lo, y_hi, my_global, row_offset, dst, cap, nout);
   int64_t c = 0;
   TRY(band_positions(h, y_lo, y_hi, &c));
@@ -2152,6 +2187,7 @@ int do_band_extract(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_
 
 template <class T, bool MIXED>
 int do_band_keep(pbpic_handle* h, int y_lo, int y_hi) {
+  TRY(materialize(h));
   int64_t c = 0;
   TRY(band_positions(h, y_lo, y_hi, &c));
   const int b = h->cur, o = 1 - b;
@@ -2168,6 +2204,7 @@ int do_band_keep(pbpic_handle* h, int y_lo, int y_hi) {
 
 template <class T, bool MIXED>
 int do_band_append(pbpic_handle* h, const void* src, int64_t n, int my_global, int row_offset) {
+  TRY(materialize(h));
   if (n < 0) return fail(PBPIC_EINVAL, "negative count");
   if (h->n + n > h->cap) return fail(PBPIC_ECAPACITY, "appending the band exceeds the capacity");
   if (n == 0) return PBPIC_OK;
@@ -2195,6 +2232,7 @@ int do_band_append(pbpic_handle* h, const void* src, int64_t n, int my_global, i
 template <class T, bool MIXED>
 int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_t nb, int off_bottom,
                     const void* top, int64_t nt, int off_top, int my_global) {
+  TRY(materialize(h));
   if (!h->sorted) {
     TRY((do_band_keep<T, MIXED>(h, y_lo, y_hi)));
     TRY((do_band_append<T, MIXED>(h, bot, nb, my_global, off_bottom)));
@@ -2294,6 +2332,7 @@ int do_field_rows(pbpic_handle* h, int j0, int nrows, void* buf, bool set) {
 
 template <class T, bool MIXED>
 int do_energies_rows(pbpic_handle* h, int y_lo, int y_hi, int wall_lo, int wall_hi, double* out) {
+  TRY(materialize(h));
   const pbpic_config& c = h->cfg;
   if (y_lo < 0 || y_hi > h->S || y_lo > y_hi) return fail(PBPIC_EINVAL, "rows outside 0..my");
   cudaStream_t s = h->stream;
