@@ -578,16 +578,16 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           }
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 4; ++j) {  // the input is not written by this launch: read-only loads
           const int p = q + j;
           const bool act = p >= pbeg && p < pend;
           const int e = sidx[j];
-          cw[j] = act ? a.cell[e] : 0u;
-          px[j] = act ? a.dx[e] : T(0);
-          py[j] = act ? a.dy[e] : T(0);
-          pux[j] = act ? a.ux[e] : T(0);
-          puy[j] = act ? a.uy[e] : T(0);
-          puz[j] = act ? a.uz[e] : T(0);
+          cw[j] = act ? __ldg(a.cell + e) : 0u;
+          px[j] = act ? __ldg(a.dx + e) : T(0);
+          py[j] = act ? __ldg(a.dy + e) : T(0);
+          pux[j] = act ? __ldg(a.ux + e) : T(0);
+          puy[j] = act ? __ldg(a.uy + e) : T(0);
+          puz[j] = act ? __ldg(a.uz + e) : T(0);
         }
       } else if (full) {
         ld4(a.cell + q, cw);
@@ -785,7 +785,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int p = q + j;
-          if (p >= pbeg && p < pend) a.pid_o[p] = a.pid_i[sidx[j]];
+          if (p >= pbeg && p < pend) a.pid_o[p] = __ldg(a.pid_i + sidx[j]);
         }
       }
     }
