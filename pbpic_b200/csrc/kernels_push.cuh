@@ -892,7 +892,7 @@ __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINB
 
 // Batched domains: persistent blocks take (domain, tile) pairs from a global
 // counter (reset to 0 before each launch) in the order of `tiles`.
-template <class T, bool MIXED, bool HIST, int G, bool COMPAT>
+template <class T, bool MIXED, bool HIST, int G, bool COMPAT, bool GATHER = false>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
     k_push_batched(const PushParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -907,7 +907,7 @@ __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINB
     const int2 it = tiles[t];
     if (threadIdx.x == 0) a = descs[it.x];
     __syncthreads();
-    push_tile<T, MIXED, HIST, G, COMPAT>(a, it.y, sm, smem_raw);
+    push_tile<T, MIXED, HIST, G, COMPAT, GATHER>(a, it.y, sm, smem_raw);
     __syncthreads();
   }
 }

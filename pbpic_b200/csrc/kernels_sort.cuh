@@ -424,108 +424,21 @@ struct ScatterParams {
   int mx, my, ybc, ty, tpc, nb;
   const int32_t* tile_off;  // position ranges of the tiles (those the push used)
   const int32_t* base;      // [ntiles][nb]
-  const uint32_t* ci;
-  const T *dxi, *dyi, *uxi, *uyi, *uzi;
-  const int32_t* pidi;
-  uint32_t* co;
-  T *dxo, *dyo, *uxo, *uyo, *uzo;
-  int32_t* pido;
+  const uint32_t* ci;       // the pushed particles' cell words
+  int32_t* perm;            // sorted slot -> element of ci
 };
 
-#ifndef PBPIC_SCATTER_IPT
-#define PBPIC_SCATTER_IPT 8
-#endif
-constexpr int SC_IPT = PBPIC_SCATTER_IPT, SC_CHUNK = 256 * SC_IPT, SC_MAXNB = 3 * (64 + 2) + 1;
+constexpr int SC_MAXNB = 3 * (64 + 2) + 1;  // window bins of the largest tile, plus a sentinel
 
-// Stable scatter of one tile. Warp w owns the chunk range
-// [w*32*SC_IPT, (w+1)*32*SC_IPT), item k of lane l at k*32 + l, so
-// (warp, item, lane) order is array order. All loads of a chunk are issued
-// before the ranking so that they overlap.
+// Per-warp bin counts and the block's running ranks of one tile.
 struct ScatterSmem {
   int32_t cnt[8][SC_MAXNB];
   int32_t run[SC_MAXNB], sbase[SC_MAXNB];
 };
 
-template <class T>
-__device__ __forceinline__ void scatter_tile(const ScatterParams<T>& a, const int t, ScatterSmem& sm) {
-  int32_t(&cnt)[8][SC_MAXNB] = sm.cnt;
-  int32_t* run = sm.run;
-  int32_t* sbase = sm.sbase;
-  const int ixt = t / a.tpc, y0 = (t - ixt * a.tpc) * a.ty, y1 = min(y0 + a.ty, a.my);
-  const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
-  const int w = threadIdx.x >> 5;
-  const unsigned lane = lane_id(), lt = lanemask_lt();
-  for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
-    run[b] = 0;
-    sbase[b] = a.base[(int64_t)t * a.nb + b];
-  }
-  for (int c0 = pbeg; c0 < pend; c0 += SC_CHUNK) {
-    for (int e = threadIdx.x; e < 8 * SC_MAXNB; e += blockDim.x) (&cnt[0][0])[e] = 0;
-    __syncthreads();
-    int bin[SC_IPT], pos[SC_IPT];
-    uint32_t vc[SC_IPT];
-    T vdx[SC_IPT], vdy[SC_IPT], vux[SC_IPT], vuy[SC_IPT], vuz[SC_IPT];
-    int32_t vpid[SC_IPT];
-    // issue every load of the chunk before ranking (memory-level parallelism)
-#pragma unroll
-    for (int k = 0; k < SC_IPT; ++k) {
-      const int p = c0 + w * (32 * SC_IPT) + k * 32 + (int)lane;
-      const bool ok = p < pend;
-      vc[k] = ok ? a.ci[p] : 0u;
-      vdx[k] = ok ? a.dxi[p] : T(0);
-      vdy[k] = ok ? a.dyi[p] : T(0);
-      vux[k] = ok ? a.uxi[p] : T(0);
-      vuy[k] = ok ? a.uyi[p] : T(0);
-      vuz[k] = ok ? a.uzi[p] : T(0);
-      vpid[k] = (ok && a.pidi) ? a.pidi[p] : 0;
-    }
-#pragma unroll
-    for (int k = 0; k < SC_IPT; ++k) {
-      const int p = c0 + w * (32 * SC_IPT) + k * 32 + (int)lane;
-      int b = a.nb;  // sentinel: beyond the tile
-      if (p < pend) {
-        b = window_bin(cw_ix(vc[k]), cw_iy(vc[k]), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
-        if (b < 0) b = a.nb;  // cannot happen: the push kept every particle in its window
-      }
-      const unsigned peers = __match_any_sync(FULL, b);
-      const int before = cnt[w][b];
-      __syncwarp();
-      if ((peers & lt) == 0) cnt[w][b] = before + __popc(peers);
-      __syncwarp();
-      pos[k] = before + __popc(peers & lt);
-      bin[k] = b;
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
-      int32_t r = run[b];
-#pragma unroll
-      for (int ww = 0; ww < 8; ++ww) {
-        const int32_t c = cnt[ww][b];
-        cnt[ww][b] = r;
-        r += c;
-      }
-      run[b] = r;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < SC_IPT; ++k) {
-      if (bin[k] < a.nb) {
-        const int64_t d = (int64_t)sbase[bin[k]] + cnt[w][bin[k]] + pos[k];
-        a.co[d] = vc[k];
-        a.dxo[d] = vdx[k];
-        a.dyo[d] = vdy[k];
-        a.uxo[d] = vux[k];
-        a.uyo[d] = vuy[k];
-        a.uzo[d] = vuz[k];
-        if (a.pido) a.pido[d] = vpid[k];
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // ------------------------------------------------- permutation-only sort
-// The same stable ranking as scatter_tile, reading only the cell words: the
+// The stable ranking of a tile's particles by new cell (warp match_any +
+// per-warp counters, array order), from the cell words only: the
 // particle at array element p of the tile gets its sorted slot d, and
 // perm[d] = p. The particle data stay where they are; the next push reads
 // them through perm (PushParams::src), and a gather (k_gather) applies perm
@@ -533,10 +446,9 @@ __device__ __forceinline__ void scatter_tile(const ScatterParams<T>& a, const in
 constexpr int SP_IPT = 8, SP_CHUNK = 256 * SP_IPT;
 
 template <class T>
-__global__ void __launch_bounds__(256) k_fused_perm(ScatterParams<T> a, int32_t* perm) {
-  __shared__ ScatterSmem sm;
+__device__ __forceinline__ void perm_tile(const ScatterParams<T>& a, const int t, ScatterSmem& sm) {
   int32_t(&cnt)[8][SC_MAXNB] = sm.cnt;
-  const int t = blockIdx.x;
+  int32_t* perm = a.perm;
   const int ixt = t / a.tpc, y0 = (t - ixt * a.tpc) * a.ty, y1 = min(y0 + a.ty, a.my);
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
   const int w = threadIdx.x >> 5;
@@ -594,10 +506,22 @@ __global__ void __launch_bounds__(256) k_fused_perm(ScatterParams<T> a, int32_t*
   }
 }
 
-// Batched domains: persistent blocks take (domain, tile) pairs from a counter.
+template <class T>
+__global__ void __launch_bounds__(256) k_fused_perm(ScatterParams<T> a) {
+  __shared__ ScatterSmem sm;
+  perm_tile(a, blockIdx.x, sm);
+}
+
+// The identity permutation: arrays already in cell order, read through perm.
+static __global__ void k_iota(int32_t* perm, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    perm[i] = (int32_t)i;
+}
+
+// Batched permutation-only sort: persistent blocks over the (domain, tile) table.
 template <class T>
 __global__ void __launch_bounds__(256)
-    k_fused_scatter_batched(const ScatterParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
+    k_fused_perm_batched(const ScatterParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
   __shared__ ScatterSmem sm;
   __shared__ ScatterParams<T> a;
   __shared__ int next;
@@ -609,7 +533,7 @@ __global__ void __launch_bounds__(256)
     const int2 it = tiles[t];
     if (threadIdx.x == 0) a = descs[it.x];
     __syncthreads();
-    scatter_tile(a, it.y, sm);
+    perm_tile(a, it.y, sm);
     __syncthreads();
   }
 }

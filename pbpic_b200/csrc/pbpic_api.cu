@@ -543,7 +543,8 @@ int do_fused_sort(pbpic_handle* h) {
   sp.ci = h->cell[h->cur];
   if (n > 0) {  // the sorted order as a permutation; the particle data stay in place
     if (!h->perm) TRY(dalloc(h, &h->perm, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
-    k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp, h->perm);
+    sp.perm = h->perm;
+    k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp);
     CKLAUNCH("k_fused_perm");
     h->lazy = true;
   }
@@ -1377,7 +1378,7 @@ extern "C" int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t 
 //   k_batch_begin          zero the current accumulators, reset counters
 //   k_push_batched         persistent blocks over the (domain, tile) table
 //   k_fused_counts_batched, k_scan_batched, k_fused_base_batched,
-//   k_fused_scatter_batched (persistent), k_tile_off_batched
+//   k_fused_perm_batched (persistent), k_tile_off_batched
 //                          the fused counting sort of every domain
 //   k_bhalf/k_efull/k_bhalf/k_nodes_batched, k_energy_rows_batched
 // Two consecutive steps (the particle buffers swap each step) are captured
@@ -1533,13 +1534,13 @@ int batch_layout(pbpic_batch* b) {
   int per_sm = 1;
   b->compat = false;
   for (pbpic_handle* h : b->dom) b->compat |= h->cfg.compat != 0;
-  const void* fn = b->groups == 1 ? (b->compat ? (const void*)k_push_batched<float, true, true, 1, true>
-                                               : (const void*)k_push_batched<float, true, true, 1, false>)
-                                  : (b->compat ? (const void*)k_push_batched<float, true, true, 2, true>
-                                               : (const void*)k_push_batched<float, true, true, 2, false>);
+  const void* fn = b->groups == 1 ? (b->compat ? (const void*)k_push_batched<float, true, true, 1, true, true>
+                                               : (const void*)k_push_batched<float, true, true, 1, false, true>)
+                                  : (b->compat ? (const void*)k_push_batched<float, true, true, 2, true, true>
+                                               : (const void*)k_push_batched<float, true, true, 2, false, true>);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PushThreads<float>::value, smem));
   b->push_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_scatter_batched<float>, 256, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_perm_batched<float>, 256, 0));
   b->scatter_blocks = std::max(1, std::min(b->ntiles, sms * std::max(1, per_sm)));
   b->gx_zero = grid_for(maxacc, 256, 1024);
   b->gx_cells = grid_for(maxcells, 256);
@@ -1564,12 +1565,23 @@ int batch_descriptors(pbpic_batch* b) {
   for (int d = 0; d < D; ++d) {
     pbpic_handle* h = b->dom[d];
     const int cur0 = h->cur;
-    for (int par = 0; par < 2; ++par) {
+    for (int par = 0; par < 2; ++par) {  // step of parity par: push i -> o through perm, then rank o
       h->cur = par == 0 ? cur0 : 1 - cur0;
-      b->h_push[par * D + d] = push_params<float, true>(h);
-      if (!b->h_push[par * D + d].cell_off) return fail(PBPIC_EINVAL, "batched push: no cell offsets");
+      PushParams<float>& pp = b->h_push[par * D + d];
+      pp = push_params<float, true>(h);
+      if (!pp.cell_off) return fail(PBPIC_EINVAL, "batched push: no cell offsets");
       const int i = h->cur, o = 1 - i;
+      pp.src = h->perm;
+      pp.cell_o = h->cell[o];
+      pp.dx_o = P<float>(h, o, 0);
+      pp.dy_o = P<float>(h, o, 1);
+      pp.ux_o = P<float>(h, o, 2);
+      pp.uy_o = P<float>(h, o, 3);
+      pp.uz_o = P<float>(h, o, 4);
+      pp.pid_i = h->pid[i];
+      pp.pid_o = h->pid[o];
       ScatterParams<float>& sp = b->h_scat[par * D + d];
+      sp = ScatterParams<float>{};
       sp.mx = h->cfg.mx;
       sp.my = h->cfg.my;
       sp.ybc = h->cfg.ybc;
@@ -1578,20 +1590,8 @@ int batch_descriptors(pbpic_batch* b) {
       sp.nb = h->nb;
       sp.tile_off = h->tile_off;
       sp.base = h->tbase;
-      sp.ci = h->cell[i];
-      sp.dxi = P<float>(h, i, 0);
-      sp.dyi = P<float>(h, i, 1);
-      sp.uxi = P<float>(h, i, 2);
-      sp.uyi = P<float>(h, i, 3);
-      sp.uzi = P<float>(h, i, 4);
-      sp.pidi = h->pid[i];
-      sp.co = h->cell[o];
-      sp.dxo = P<float>(h, o, 0);
-      sp.dyo = P<float>(h, o, 1);
-      sp.uxo = P<float>(h, o, 2);
-      sp.uyo = P<float>(h, o, 3);
-      sp.uzo = P<float>(h, o, 4);
-      sp.pido = h->pid[o];
+      sp.ci = h->cell[o];
+      sp.perm = h->perm;
     }
     h->cur = cur0;
     FusedSortParams& f = b->h_fsort[d];
@@ -1651,13 +1651,13 @@ int batch_enqueue_step(pbpic_batch* b, int par) {
   const PushParams<float>* pp = b->d_push + (size_t)par * D;
   const unsigned nt = PushThreads<float>::value;
   if (b->groups == 1 && b->compat)
-    k_push_batched<float, true, true, 1, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 1, true, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   else if (b->groups == 1)
-    k_push_batched<float, true, true, 1, false><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 1, false, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   else if (b->compat)
-    k_push_batched<float, true, true, 2, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 2, true, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   else
-    k_push_batched<float, true, true, 2, false><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
+    k_push_batched<float, true, true, 2, false, true><<<b->push_blocks, nt, b->push_smem, s>>>(pp, b->d_tiles, b->ntiles, ctr);
   CKLAUNCH("k_push_batched");
   k_fused_counts_batched<<<dim3(b->gx_cells, D), 256, 0, s>>>(b->d_fsort);
   CKLAUNCH("k_fused_counts_batched");
@@ -1665,9 +1665,9 @@ int batch_enqueue_step(pbpic_batch* b, int par) {
   CKLAUNCH("k_scan_batched");
   k_fused_base_batched<<<dim3(b->gx_bins, D), 256, 0, s>>>(b->d_fsort);
   CKLAUNCH("k_fused_base_batched");
-  k_fused_scatter_batched<float><<<b->scatter_blocks, 256, 0, s>>>(b->d_scat + (size_t)par * D, b->d_tiles,
-                                                                   b->ntiles, ctr + 1);
-  CKLAUNCH("k_fused_scatter_batched");
+  k_fused_perm_batched<float><<<b->scatter_blocks, 256, 0, s>>>(b->d_scat + (size_t)par * D, b->d_tiles,
+                                                                b->ntiles, ctr + 1);
+  CKLAUNCH("k_fused_perm_batched");
   k_tile_off_batched<<<dim3(b->gx_tiles, D), 256, 0, s>>>(b->d_toff);
   CKLAUNCH("k_tile_off_batched");
   k_bhalf_batched<float><<<dim3(b->gx_field, D), 256, 0, s>>>(b->d_field);
@@ -1724,9 +1724,19 @@ int batch_step(pbpic_batch* b, int nsteps) {
   if (nsteps <= 0) return PBPIC_OK;
   for (pbpic_handle* h : b->dom)
     if (h->filters) return fail(PBPIC_EINVAL, "the batched form does not apply field filters");
+  // Every batched step reads through the domain's permutation (the push) and
+  // writes a new one (the sort): a domain whose arrays are already in cell
+  // order enters with the identity.
   for (pbpic_handle* h : b->dom) {
-    TRY(materialize(h));
     if (!h->sorted) TRY(do_sort<float, true>(h));
+    if (!h->perm) TRY(dalloc(h, &h->perm, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
+    if (!h->lazy) {
+      if (h->n > 0) {
+        k_iota<<<grid_for(h->n, 256), 256, 0, h->stream>>>(h->perm, h->n);
+        CKLAUNCH("k_iota");
+      }
+      h->lazy = true;
+    }
     TRY(ensure_hist(h, h->itime + nsteps + 2));
   }
   TRY(batch_descriptors(b));
@@ -1742,6 +1752,7 @@ int batch_step(pbpic_batch* b, int nsteps) {
     h->itime += nsteps;
     h->sorted = true;
     h->hist_valid = false;
+    h->lazy = true;  // the last step's permutation
   }
   return PBPIC_OK;
 }
