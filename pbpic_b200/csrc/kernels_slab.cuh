@@ -12,7 +12,8 @@
 // and, when the particles are sorted by cell, single-pass versions: a band
 // copied column by column from the cell offsets (k_band_out_sorted), and the
 // own rows merged with both received bands straight into cell order
-// (k_band_assemble).
+// (k_band_assemble); both read through the sort's permutation when the
+// particle arrays are held in permuted order.
 #pragma once
 #include "device_common.cuh"
 #include "kernels_misc.cuh"
@@ -207,10 +208,12 @@ __device__ __forceinline__ int column_of(const int32_t* start, int mx, int64_t k
 template <class T, class R>
 __global__ void k_band_out_sorted(int64_t total, const int32_t* colstart, const int32_t* off, int mx, int my, int y_lo,
                                   const uint32_t* cell, const T* dx, const T* dy, const T* ux, const T* uy,
-                                  const T* uz, const int32_t* pid, int my_global, int row_offset, RefRec<R>* out) {
+                                  const T* uz, const int32_t* pid, int my_global, int row_offset, RefRec<R>* out,
+                                  const int32_t* perm) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
     const int ix = column_of(colstart, mx, k);
-    const int64_t i = (int64_t)off[(int64_t)ix * my + y_lo] + (k - colstart[ix]);
+    const int64_t j = (int64_t)off[(int64_t)ix * my + y_lo] + (k - colstart[ix]);  // sorted position
+    const int64_t i = perm ? (int64_t)perm[j] : j;
     const uint32_t w = cell[i];
     RefRec<R> r;
     r.dx = (R)dx[i];
@@ -271,13 +274,14 @@ template <class T, class R>
 __global__ void k_band_assemble(int64_t total, ReplaceSrc s, const RefRec<R>* bot, const RefRec<R>* top,
                                 const uint32_t* ci, const T* dxi, const T* dyi, const T* uxi, const T* uyi,
                                 const T* uzi, const int32_t* pidi, uint32_t* co, T* dxo, T* dyo, T* uxo, T* uyo,
-                                T* uzo, int32_t* pido, int* status) {
+                                T* uzo, int32_t* pido, int* status, const int32_t* perm) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
     const int ix = column_of(s.outstart, s.mx, k);
     int64_t r = k - s.outstart[ix];
     const int nb = s.bcnt[ix], no = s.ocnt[ix];
-    if (r >= nb && r < nb + no) {  // own particle
-      const int64_t i = (int64_t)s.off[(int64_t)ix * s.my + s.y_lo] + (r - nb);
+    if (r >= nb && r < nb + no) {  // own particle (read through the sort's permutation when there is one)
+      const int64_t j = (int64_t)s.off[(int64_t)ix * s.my + s.y_lo] + (r - nb);
+      const int64_t i = perm ? (int64_t)perm[j] : j;
       co[k] = ci[i];
       dxo[k] = dxi[i];
       dyo[k] = dyi[i];

@@ -2168,7 +2168,8 @@ int band_extract_sorted(pbpic_handle* h, int y_lo, int y_hi, int my_global, int 
   if (total > 0) {
     k_band_out_sorted<T, T><<<grid_for(total, 256), 256, 0, s>>>(
         total, colstart, h->off, mx, h->cfg.my, y_lo, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
-        P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], my_global, row_offset, (RefRec<T>*)dst);
+        P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], my_global, row_offset, (RefRec<T>*)dst,
+        h->lazy ? h->perm : nullptr);
     CKLAUNCH("k_band_out_sorted");
   }
   CK(cudaStreamSynchronize(s));
@@ -2178,8 +2179,8 @@ int band_extract_sorted(pbpic_handle* h, int y_lo, int y_hi, int my_global, int 
 template <class T, bool MIXED>
 int do_band_extract(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_offset, void* dst, int64_t cap,
                     int64_t* nout) {
-  TRY(materialize(h));
   if (h->sorted) return band_extract_sorted<T, MIXED>(h, y_lo, y_hi, my_global, row_offset, dst, cap, nout);
+  TRY(materialize(h));
   int64_t c = 0;
   TRY(band_positions(h, y_lo, y_hi, &c));
   if (nout) *nout = c;
@@ -2243,8 +2244,7 @@ int do_band_append(pbpic_handle* h, const void* src, int64_t n, int my_global, i
 template <class T, bool MIXED>
 int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_t nb, int off_bottom,
                     const void* top, int64_t nt, int off_top, int my_global) {
-  TRY(materialize(h));
-  if (!h->sorted) {
+  if (!h->sorted) {  // (a handle in permuted order is sorted: the path below reads through the permutation)
     TRY((do_band_keep<T, MIXED>(h, y_lo, y_hi)));
     TRY((do_band_append<T, MIXED>(h, bot, nb, my_global, off_bottom)));
     TRY((do_band_append<T, MIXED>(h, top, nt, my_global, off_top)));
@@ -2300,10 +2300,11 @@ int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_
     k_band_assemble<T, T><<<grid_for(total, 256), 256, 0, s>>>(
         total, rs, (const RefRec<T>*)bot, (const RefRec<T>*)top, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
         P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], h->cell[o], P<T>(h, o, 0), P<T>(h, o, 1),
-        P<T>(h, o, 2), P<T>(h, o, 3), P<T>(h, o, 4), h->pid[o], h->status);
+        P<T>(h, o, 2), P<T>(h, o, 3), P<T>(h, o, 4), h->pid[o], h->status, h->lazy ? h->perm : nullptr);
     CKLAUNCH("k_band_assemble");
   }
   h->cur = o;
+  h->lazy = false;  // the assembled arrays are in cell order themselves
   h->n = total;
   // cell offsets and tile ranges of the new (sorted) array
   CK(cudaMemsetAsync(h->counts, 0, (size_t)(h->ncells + 1) * 4, s));
