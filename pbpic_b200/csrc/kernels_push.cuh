@@ -463,18 +463,20 @@ struct PushSmem<float, true> {
 
 // Rare path: a particle outside its tile adds its 16 terms (staged in the
 // thread's shared-memory column, stride 33) to global memory.
+// (The geometry comes by value: a reference to the kernel's parameters would
+// make every thread copy them to local memory.)
 template <class T, bool MIXED>
-__device__ __noinline__ void deposit_global(const PushParams<T>& a, const T* col, int ix, int iy, int dcx, int dcy,
-                                            int di, int dj) {
+__device__ __noinline__ void deposit_global(void* jacc, int mx, int my, int S, int ybc, int compat, const T* col,
+                                            int ix, int iy, int dcx, int dcy, int di, int dj) {
   using Acc = typename std::conditional<MIXED, long long, double>::type;
-  Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
+  Acc* gacc = reinterpret_cast<Acc*>(jacc);
   for (int k = 0; k < 16; ++k) {
     int rx, ry;
     term_node(k, dcx, dcy, di, dj, &rx, &ry);
     long long gi;
     int sg;
     const T v = col[k * 33];
-    if (map_current(k >> 2, ix + rx, iy + ry, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
+    if (map_current(k >> 2, ix + rx, iy + ry, mx, my, S, ybc, compat, &gi, &sg))
       acc_add(&gacc[gi], to_acc<T, MIXED>(sg < 0 ? -v : v));
   }
 }
@@ -746,7 +748,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           status |= 4;
 #pragma unroll
           for (int k = 0; k < 16; ++k) mycol[k * 33] = o.e[k];
-          deposit_global<T, MIXED>(a, mycol, ix, iy, o.dcx, o.dcy, o.di, o.dj);
+          deposit_global<T, MIXED>(a.jacc, a.mx, a.my, a.S, a.ybc, a.compat, mycol, ix, iy, o.dcx, o.dcy, o.di, o.dj);
         }
         rot4(cw, o.cw);
         rot4(px, o.dx);
