@@ -84,30 +84,6 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Segmented inclusive scan across the warp (Hillis-Steele with head flags):
-// after the call, the last lane of each run of lanes that started with a head
-// holds the sum of the run. Lane order is fixed, so the result is
-// deterministic.
-template <class V, int N>
-__device__ __forceinline__ void warp_segmented_scan(V (&v)[N], unsigned head) {
-  const unsigned lane = lane_id();
-  unsigned flag = head;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    unsigned fprev = __shfl_up_sync(FULL, flag, d);
-    V t[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) t[k] = __shfl_up_sync(FULL, v[k], d);
-    if (lane >= (unsigned)d) {
-      if (!flag) {
-#pragma unroll
-        for (int k = 0; k < N; ++k) v[k] += t[k];
-      }
-      flag |= fprev;
-    }
-  }
-}
-
 // Block-wide sum of a double into thread 0 (blockDim.x a multiple of 32, <= 1024).
 __device__ __forceinline__ double block_sum(double v, double* sm /* >= 32 */) {
 #pragma unroll

@@ -16,12 +16,11 @@
 // does not cross), jz on the 3x3 nodes around the cell, rho -- forms a
 // 17-value stencil. At the end of a pass the lanes of a warp that share a
 // cell (a run of lanes: the keys do not decrease across a sorted array) are
-// summed: mixed form, each lane stages its stencil in shared memory and 17
-// lanes add up the run's columns in lane order, one stencil entry each (a
-// thread whose particles change cell keeps its first cell's part in a second
-// column, joined to the run it continues); plain form, a segmented scan across
-// the lanes. Each run's sum is added to a shared-memory window by 17 lanes at
-// once. A crossing particle adds its second segment (4 values) on its own. The window (4 node columns x tile_rows + 3 node rows) is folded
+// summed: each lane stages its stencil in shared memory and 17 lanes add up
+// the run's columns in lane order, one stencil entry each (a thread whose
+// particles change cell keeps its first cell's part in a second column, joined
+// to the run it continues). Each run's sum is added to a shared-memory window
+// by 17 lanes at once. A crossing particle adds its second segment (4 values) on its own. The window (4 node columns x tile_rows + 3 node rows) is folded
 // into the global current at the end, with the periodic wrap and the wall
 // images. Particles outside their tile (array not sorted) add straight to
 // global memory.
@@ -447,8 +446,10 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 #endif
 
 // Per-warp staging of the lanes' stencil sums (stride 33: conflict-free rows
-// and columns). The mixed form keeps a second column per lane for the first
-// cell of a lane whose particles change cell inside a pass.
+// and columns), and a second column per lane for the first cell of a lane
+// whose particles change cell inside a pass: static in the mixed form; the
+// plain form's (FP64, twice the size) is in the dynamic shared memory, after
+// the window and the histogram (push_first_offset).
 template <class T, bool MIXED>
 struct PushSmem {
   T stage[PushThreads<T>::value / 32][17][33];
@@ -505,9 +506,19 @@ __device__ __forceinline__ void rot4(V (&v)[4], V x) {
   v[3] = x;
 }
 
+// Byte offset of the plain form's second stage in the dynamic shared memory.
+__host__ __device__ __forceinline__ size_t push_first_offset(int ty) {
+  return ((size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + 15) & ~(size_t)15;
+}
+
+// Round-to-nearest add that the compiler keeps as written (no fusion into an FMA).
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
 // Push of tile t of the domain `a`, by all threads of the block. G float4
 // groups of particles per thread per pass (8 particles for G = 2).
-// smem_raw: window (16*(ty+3) accumulators) then histogram (3*(ty+2) int).
+// smem_raw: window (16*(ty+3) accumulators), histogram (3*(ty+2) int), then the
+// mixed form's crossers' windows or the plain form's second stage.
 template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true, bool GATHER = false>
 __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
                                           unsigned char* smem_raw) {
@@ -518,6 +529,12 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   int* hist = reinterpret_cast<int*>(win + 16 * WR);
   unsigned* clo = reinterpret_cast<unsigned*>(hist + NB);  // crossers: jx, jy planes (8 * WR)
   int* chi = reinterpret_cast<int*>(clo + 8 * WR);
+  // [warp][17][33] first parts of the lanes whose particles change cell (the
+  // mixed form's static array keeps its addresses constant)
+  auto first = [&](int w_, int k_, int l_) -> T& {
+    if constexpr (MIXED) return sm.first[w_][k_][l_];
+    else return reinterpret_cast<T*>(smem_raw + push_first_offset(TY))[(w_ * 17 + k_) * 33 + l_];
+  };
   const int ixt = t / a.tiles_per_col;
   const int y0 = (t - ixt * a.tiles_per_col) * TY;
   const int y1 = min(y0 + TY, a.my);
@@ -558,7 +575,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 #pragma unroll
     for (int k = 0; k < 17; ++k) acc[k] = T(0);
     int acc_key = -1;
-    int first_key = -1;  // mixed form: cell of this pass's finished first part (in sm.first), or -1
+    int first_key = -1;  // cell of this pass's finished first part (in `first`), or -1
     int cache_cell = -1;
     Node6<T> n00{}, n01{}, n10{}, n11{};
     T pke_e = T(0), pke_i = T(0);  // this pass's kinetic energy, per species
@@ -668,14 +685,12 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           const int key = iy - y0;
           if (key != acc_key) {
             if (acc_key >= 0) {  // the thread's particles changed cell
-              if constexpr (MIXED) {
-                if (first_key < 0) {  // first change of the pass: keep the part for the run sums
-                  first_key = acc_key;
+              if (first_key < 0) {  // first change of the pass: keep the part for the run sums
+                first_key = acc_key;
 #pragma unroll
-                  for (int k = 0; k < 17; ++k) {
-                    sm.first[w][k][lane] = acc[k];
-                    acc[k] = T(0);
-                  }
+                for (int k = 0; k < 17; ++k) {
+                  first(w, k, lane) = acc[k];
+                  acc[k] = T(0);
                 }
               }
               if (acc_key >= 0 && acc_key != first_key) {  // a cell wholly inside this thread's pass
@@ -797,61 +812,41 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     const int key = acc_key >= 0 ? acc_key : -1 - (int)lane;
     const int kprev = __shfl_up_sync(FULL, key, 1);
     const unsigned head = (lane == 0) || (kprev != key);
-    if constexpr (MIXED) {
-      // Keys do not decrease across the lanes, so a run is the lanes head..tail
-      // plus, when the next lane's first part has the run's cell, that part. The
-      // 17 lanes sum the run's staged columns in lane order (a fixed order: the
-      // result does not depend on timing). A first part that does not continue
-      // the run ending at the previous lane is added on its own.
-      const int fnext = __shfl_down_sync(FULL, first_key, 1);
-      const unsigned heads = __ballot_sync(FULL, head);
-      const unsigned head_next = __shfl_down_sync(FULL, head, 1);
-      unsigned tails = __ballot_sync(FULL, acc_key >= 0 && (lane == 31 || head_next));
-      const bool joined = lane > 0 && head && kprev == first_key;
-      unsigned solo = __ballot_sync(FULL, first_key >= 0 && !joined);
+    // Keys do not decrease across the lanes, so a run is the lanes head..tail
+    // plus, when the next lane's first part has the run's cell, that part. The
+    // 17 lanes sum the run's staged columns in lane order (a fixed order: the
+    // result does not depend on timing). A first part that does not continue
+    // the run ending at the previous lane is added on its own.
+    const int fnext = __shfl_down_sync(FULL, first_key, 1);
+    const unsigned heads = __ballot_sync(FULL, head);
+    const unsigned head_next = __shfl_down_sync(FULL, head, 1);
+    unsigned tails = __ballot_sync(FULL, acc_key >= 0 && (lane == 31 || head_next));
+    const bool joined = lane > 0 && head && kprev == first_key;
+    unsigned solo = __ballot_sync(FULL, first_key >= 0 && !joined);
 #pragma unroll
-      for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
-      __syncwarp();
-      while (tails) {
-        const int src = __ffs(tails) - 1;
-        tails &= tails - 1;
-        const int start = 31 - __clz(heads & (0xffffffffu >> (31 - src)));
-        const int kt = __shfl_sync(FULL, key, src);
-        const int nf = __shfl_sync(FULL, fnext, src);
-        if (lane < 17) {
-          const T* row = &sm.stage[w][lane][0];
-          T v = row[start];
-          for (int l = start + 1; l <= src; ++l) v = __fadd_rn(v, row[l]);
-          if (src < 31 && nf == kt) v = __fadd_rn(v, sm.first[w][lane][src + 1]);
-          if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
-        }
+    for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
+    __syncwarp();
+    while (tails) {
+      const int src = __ffs(tails) - 1;
+      tails &= tails - 1;
+      const int start = 31 - __clz(heads & (0xffffffffu >> (31 - src)));
+      const int kt = __shfl_sync(FULL, key, src);
+      const int nf = __shfl_sync(FULL, fnext, src);
+      if (lane < 17) {
+        const T* row = &sm.stage[w][lane][0];
+        T v = row[start];
+        for (int l = start + 1; l <= src; ++l) v = add_rn(v, row[l]);
+        if (src < 31 && nf == kt) v = add_rn(v, first(w, lane, src + 1));
+        if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
       }
-      while (solo) {
-        const int src = __ffs(solo) - 1;
-        solo &= solo - 1;
-        const int kt = __shfl_sync(FULL, first_key, src);
-        if (lane < 17) {
-          const T v = sm.first[w][lane][src];
-          if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
-        }
-      }
-    } else {
-      // plain form: segmented scan across the lanes; each run's tail holds its sum
-      warp_segmented_scan<T, 17>(acc, head);
-      const unsigned head_next = __shfl_down_sync(FULL, head, 1);
-      const bool tail = acc_key >= 0 && (lane == 31 || head_next);
-#pragma unroll
-      for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
-      __syncwarp();
-      unsigned tails = __ballot_sync(FULL, tail);
-      while (tails) {
-        const int src = __ffs(tails) - 1;
-        tails &= tails - 1;
-        const int kt = __shfl_sync(FULL, key, src);
-        if (lane < 17) {
-          const T v = sm.stage[w][lane][src];
-          if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
-        }
+    }
+    while (solo) {
+      const int src = __ffs(solo) - 1;
+      solo &= solo - 1;
+      const int kt = __shfl_sync(FULL, first_key, src);
+      if (lane < 17) {
+        const T v = first(w, lane, src);
+        if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
       }
     }
     __syncwarp();  // the stage is rewritten in the next pass

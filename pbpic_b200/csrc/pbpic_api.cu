@@ -167,6 +167,7 @@ struct pbpic_handle {
   // particle arrays applies it first (materialize).
   int32_t* perm = nullptr;
   bool lazy = false;
+  size_t push_optin = 0;    // dynamic shared memory the plain form's k_push may take
   int nb = 0;               // window bins per tile, 3*(TY+2)
   int tile_cap = 0;         // tiles the per-tile arrays hold
   int64_t bin_cap = 0;      // (tile, bin) entries tilecnt and tbase hold
@@ -212,10 +213,31 @@ int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
 
 // Dynamic shared memory of k_push: the tile's current window (16 x (ty+3)
 // 8-byte accumulators), the new-cell histogram (3 x (ty+2) int) and, in the
-// mixed form, the crossers' split 32-bit windows (2 x 8 x (ty+3)). With the
-// static part this stays below the 48 KB a launch gets without opting in.
+// mixed form, the crossers' split 32-bit windows (2 x 8 x (ty+3)); with the
+// static part this stays below the 48 KB a launch gets without opting in. The
+// plain form adds the second stage of its run sums (8 warps x 17 x 33 doubles),
+// which takes it above 48 KB (push_smem_optin).
 size_t push_smem_bytes(int ty, bool mixed) {
-  return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (mixed ? (size_t)16 * (ty + 3) * 4 : 0);
+  if (!mixed) return push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * sizeof(double);
+  return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4;
+}
+
+// Lets the plain form's k_push instantiations take more than 48 KB of shared
+// memory. The limit belongs to the function and every handle on the device
+// shares it, so it is set to what the tallest tile (64 rows) needs, never to a
+// handle's own smaller figure (once per handle: a handle stays on one device).
+template <class T, bool MIXED>
+int push_smem_optin(pbpic_handle* h) {
+  if constexpr (!MIXED) {
+    const size_t smem = push_smem_bytes(64, false);
+    if (h->push_optin >= smem) return PBPIC_OK;
+    const void* fns[] = {(const void*)k_push<T, MIXED, true, false, true>, (const void*)k_push<T, MIXED, true, true, true>,
+                         (const void*)k_push<T, MIXED, true, false>,       (const void*)k_push<T, MIXED, true, true>,
+                         (const void*)k_push<T, MIXED, false, false>,      (const void*)k_push<T, MIXED, false, true>};
+    for (const void* f : fns) CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    h->push_optin = smem;
+  }
+  return PBPIC_OK;
 }
 
 int ensure_staging(pbpic_handle* h, size_t bytes) {
@@ -467,6 +489,8 @@ int do_push(pbpic_handle* h) {
   CK(cudaMemsetAsync(h->jacc, 0, (size_t)4 * plane_elems(h) * 8, s));
   PushParams<T> p = push_params<T, MIXED>(h);
   const size_t smem = push_smem_bytes(h->TY, MIXED);
+  if (h->TY > 64) return fail(PBPIC_ESTATE, "k_push: tiles have at most 64 rows");
+  TRY((push_smem_optin<T, MIXED>(h)));
   const bool hist = h->sorted && h->fused_ok;
   if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
   const int nt = PushThreads<T>::value;

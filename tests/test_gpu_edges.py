@@ -214,3 +214,28 @@ def test_readers_after_a_permuted_sort(gpu_lib, precision, tmp_path):
     assert abs(ga - gb) <= 1e-12  # a small difference of O(1) terms, summed with FP64 atomics
     assert np.array_equal(sa, sb) and np.array_equal(ca, cb)
     assert np.array_equal(ca, np.bincount(pa["grid"] - 1, minlength=cfg["mx"] * cfg["my"]))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_handles_of_different_tile_heights(gpu_lib, precision):
+    """Handles on one device whose tiles differ in height step in turn: the
+    push's shared-memory size is a limit of the kernel function, which every
+    handle shares (the plain form's exceeds the 48 KB a launch gets without
+    opting in), so a handle with short tiles must not lower it below another's.
+    The runs agree (FP64: within 1e-12, the order of the atomic current sums)."""
+    cfg, ld = configs.harris(32, 80, 8, seed=3)
+    n = pbpic_b200.Simulation(**cfg, precision=precision, capacity=1).loader_count(**ld)
+    sims = [pbpic_b200.Simulation(**cfg, precision=precision, capacity=n, track_pid=True, tile_rows=ty)
+            for ty in (64, 4, 16)]
+    try:
+        for s in sims:
+            s.init_plasma(**ld)
+        for _ in range(3):
+            for s in sims:
+                s.step(1, sort_every=1)
+        ps = [s.particles() for s in sims]
+        for p in ps[1:]:
+            assert_particles(p, ps[0], 1e-12 if precision == "fp64" else 2e-5)
+    finally:
+        for s in sims:
+            s.close()
