@@ -430,8 +430,11 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 }
 
 // Compile-time shape of the push loop: particles per thread per pass are
-// 4 * PBPIC_PUSH_HALVES (read as float4 groups), and PBPIC_PUSH_UNROLL selects
-// whether the loop over the 4 particles of a group is unrolled.
+// 4 * PBPIC_PUSH_HALVES (read as float4 groups; PBPIC_PUSH_HALVES_FP64 for the
+// plain form, where 4 particles a pass measured 1 % faster than 8 at three
+// blocks per SM), PBPIC_PUSH_UNROLL selects whether the loop over the 4
+// particles of a group is unrolled, and the MINBLOCKS values are the resident
+// blocks per SM the register allocation must allow.
 #ifndef PBPIC_PUSH_HALVES
 #define PBPIC_PUSH_HALVES 2
 #endif
@@ -440,6 +443,12 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 #endif
 #ifndef PBPIC_PUSH_MINBLOCKS
 #define PBPIC_PUSH_MINBLOCKS 4
+#endif
+#ifndef PBPIC_PUSH_HALVES_FP64
+#define PBPIC_PUSH_HALVES_FP64 1
+#endif
+#ifndef PBPIC_PUSH_MINBLOCKS_FP64
+#define PBPIC_PUSH_MINBLOCKS_FP64 3
 #endif
 #ifndef PBPIC_PUSH_NODECACHE
 #define PBPIC_PUSH_NODECACHE 0
@@ -881,16 +890,16 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 // set; GATHER when the input is the previous step's arrays and the sort's
 // permutation.
 template <class T, bool MIXED, bool HIST, bool COMPAT, bool GATHER = false>
-__global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1) k_push(PushParams<T> a) {
+__global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : PBPIC_PUSH_MINBLOCKS_FP64) k_push(PushParams<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T, MIXED> sm;
-  push_tile<T, MIXED, HIST, PBPIC_PUSH_HALVES, COMPAT, GATHER>(a, blockIdx.x, sm, smem_raw);
+  push_tile<T, MIXED, HIST, MIXED ? PBPIC_PUSH_HALVES : PBPIC_PUSH_HALVES_FP64, COMPAT, GATHER>(a, blockIdx.x, sm, smem_raw);
 }
 
 // Batched domains: persistent blocks take (domain, tile) pairs from a global
 // counter (reset to 0 before each launch) in the order of `tiles`.
 template <class T, bool MIXED, bool HIST, int G, bool COMPAT, bool GATHER = false>
-__global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : 1)
+__global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : PBPIC_PUSH_MINBLOCKS_FP64)
     k_push_batched(const PushParams<T>* descs, const int2* tiles, int ntiles, int* counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T, MIXED> sm;
