@@ -8,17 +8,22 @@ namespace pbd {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int NTHREADS = 256;  // threads per block of the particle kernels
 
-// Threads per block of the push: FP32 (mixed) 128, four blocks per SM (finer
-// passes over a tile than two blocks of 256, 1.4 % faster step); FP64 (plain)
+// Threads per block of the push: FP32 (mixed) 128, five blocks per SM at 96
+// registers (finer passes over a tile than two blocks of 256, 1.4 % faster
+// step; 20 warps per SM against 16 at four blocks: 1.6 % faster single-domain
+// step, 4.3 % faster batched step, with 84 B spilled); FP64 (plain)
 // 128, three blocks per SM at 168 registers (12 warps per SM, against 8 for one
 // 256-thread block at the 196 registers the kernel takes uncapped: a 23 % shorter
 // step, with 4 bytes spilled).
+#ifndef PBPIC_PUSH_THREADS_FP32
+#define PBPIC_PUSH_THREADS_FP32 128
+#endif
 #ifndef PBPIC_PUSH_THREADS_FP64
 #define PBPIC_PUSH_THREADS_FP64 128
 #endif
 template <class T>
 struct PushThreads {
-  static constexpr int value = sizeof(T) == 4 ? 128 : PBPIC_PUSH_THREADS_FP64;
+  static constexpr int value = sizeof(T) == 4 ? PBPIC_PUSH_THREADS_FP32 : PBPIC_PUSH_THREADS_FP64;
 };
 
 // Current components (denjr record of pic2d.f90:65-67).

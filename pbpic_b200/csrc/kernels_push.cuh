@@ -442,7 +442,7 @@ __device__ __forceinline__ typename std::conditional<MIXED, long long, double>::
 #define PBPIC_PUSH_UNROLL 0
 #endif
 #ifndef PBPIC_PUSH_MINBLOCKS
-#define PBPIC_PUSH_MINBLOCKS 4
+#define PBPIC_PUSH_MINBLOCKS 5
 #endif
 #ifndef PBPIC_PUSH_HALVES_FP64
 #define PBPIC_PUSH_HALVES_FP64 1
