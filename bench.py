@@ -33,7 +33,7 @@ METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy 
 # permutation, the permutation itself, the state written in cell order) from the ncu capture
 # summarised in profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to
 # the particles.
-PUSH_DRAM_BYTES_PER_PARTICLE = 60.4
+PUSH_DRAM_BYTES_PER_PARTICLE = 61.0
 UNIT = "particle-steps/s"
 
 
@@ -58,6 +58,24 @@ def workload(name, seed_offset=0):
     cfg, ld = configs.WORKLOADS[name]()
     ld = dict(ld, seed=ld["seed"] + seed_offset)
     return cfg, ld
+
+
+# HBM3e of an HGX B200 as specified (the roofline's denominator is the measured copy bandwidth)
+NOMINAL_HBM_GBS = 7700.0
+
+
+def host_cpu():
+    """Host threads and CPU model of the machine the CPU baseline runs on."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model}
 
 
 def measured_peak_hbm():
@@ -306,6 +324,31 @@ def run_cpu_sample(workload_name, steps, seed_offset=0):
                        "of push+fieldsolve+sort, FP64, OpenMP over all host threads")
 
 
+def run_cpu_single_f32(steps=3):
+    """One host thread of the oracle in FP32 (the reference's own precision)
+    on the 128x128 uniform plasma, 32 particles per cell per species."""
+    from oracle import oracle as O
+    from pbpic_b200 import configs
+    cfg, ld = configs.uniform_c1()
+    p, yee = O.load_plasma(cfg, ld)
+    o = O.Oracle(**cfg, precision="f32")
+    o.load_particles(p)
+    del p
+    o.set_fields(yee)
+    o.countingsort()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.pusher()
+        o.fieldsolver()
+        o.countingsort()
+    dt = time.perf_counter() - t0
+    n = o.L.orc_nptl(o.h)
+    o.close()
+    return {"value": n * steps / dt, "unit": UNIT, "cores": 1,
+            "sample": f"{cfg['mx']}x{cfg['my']} cells, {n} particles, {steps} steps of push+fieldsolve+sort, FP32, "
+                      "one thread"}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -323,7 +366,7 @@ def main():
                 "data": "synthetic: seeded Philox Harris sheet",
                 "config": {"workload": args.workload, "sample": r["sample"]},
                 "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
-                                 "sample": r["sample"]},
+                                 "sample": r["sample"], "host": host_cpu()},
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -334,6 +377,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_sample(args.workload, 4)
+        cpu["single_thread_fp32"] = run_cpu_single_f32()
     ranks.close()
     if rank != 0:
         return
@@ -357,6 +401,7 @@ def main():
                      "frac": achieved_push / peak, "traffic": PUSH_DRAM_BYTES_PER_PARTICLE * n,
                      "kernel": "k_push<float,true,true,false,true>",
                      "bytes_per_launch": bytes_push, "peak_kind": peak_kind,
+                     "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": achieved_push / NOMINAL_HBM_GBS,
                      "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak},
         "phase_ms": {"push": m["t_push"], "fieldsolve": m["t_field"], "sort": m["t_sort"]},
         "energy": {"mixed_drift": m["energy_drift"], "gauss_residual": m["gauss"], "reconnected_flux": m["flux"]},
@@ -397,7 +442,8 @@ def main():
             "weibel_gauss_residual_max": ens["gauss"], "status": ens["status"]}
     if cpu:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
-                                "sample": cpu["sample"]}
+                                "sample": cpu["sample"], "host": host_cpu(),
+                                "single_thread_fp32": cpu["single_thread_fp32"]}
     print(json.dumps(line), flush=True)
 
 
