@@ -193,6 +193,10 @@ int pbpic_cell_counts(pbpic_handle* h, int32_t* counts);
 /* Gauss's law residual max |div E / cva^2 - rho| over interior nodes, with rho
  * the CIC charge density (units of n0 e) of the current particle positions. */
 int pbpic_gauss_residual(pbpic_handle* h, double* out);
+/* The same over the node rows [y_lo, y_hi) only (a y slab's own rows; its
+ * ghost rows hold the neighbours' values). No reference counterpart: the
+ * reference has no Gauss diagnostic. */
+int pbpic_gauss_residual_rows(pbpic_handle* h, int32_t y_lo, int32_t y_hi, double* out);
 /* Reconnected flux: half the sum of |By| along the node row my/2 times dx. */
 int pbpic_reconnected_flux(pbpic_handle* h, double* out);
 /* Energy spectra (energyspectra, pic2d.f90:1957-1990): counts[0][k-1]

@@ -104,6 +104,7 @@ SIGNATURES = {
     "pbpic_time_step": [_P, _PI32],
     "pbpic_cell_counts": [_P, _P],
     "pbpic_gauss_residual": [_P, _PD],
+    "pbpic_gauss_residual_rows": [_P, _I32, _I32, _PD],
     "pbpic_reconnected_flux": [_P, _PD],
     "pbpic_status": [_P, _PI32],
     "pbpic_counting_sort_keys": [_P, _I64, _I32, _P, _P, _P],

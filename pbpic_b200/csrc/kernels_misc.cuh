@@ -132,10 +132,12 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
 // max |div E / cva^2 - in0 rho| over interior nodes; div E at node (i, j) is
 // (ex(i,j) - ex(i-1,j))/dx + (ey(i,j) - ey(i,j-1))/dy.
 template <class T>
-__global__ void k_gauss(int mx, int my, int S, int ybc, const T* ex, const T* ey, const double* rho,
-                        double idx, double idy, double icva2, double in0, double* out) {
+__global__ void k_gauss(int mx, int my, int S, int ybc, int jlo, int jhi, const T* ex, const T* ey,
+                        const double* rho, double idx, double idy, double icva2, double in0, double* out) {
   double m = 0.0;
-  const int j0 = ybc == 0 ? 0 : 1, j1 = my;  // walls: interior rows 1..my-1
+  // node rows [jlo, jhi) of 0..my-1 (walls: interior rows 1..my-1)
+  const int j0 = max(jlo, ybc == 0 ? 0 : 1), j1 = min(jhi, my);
+  if (j1 <= j0) return;
   const int rows = j1 - j0;
   const int64_t nn = (int64_t)mx * rows;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (int64_t)gridDim.x * blockDim.x) {

@@ -819,7 +819,7 @@ int do_init_plasma(pbpic_handle* h, const pbpic_loader* ld) {
 }
 
 template <class T, bool MIXED>
-int do_gauss(pbpic_handle* h, double* out) {
+int do_gauss(pbpic_handle* h, double* out, int jlo, int jhi) {
   TRY(materialize(h));
   cudaStream_t s = h->stream;
   const int64_t pe = plane_elems(h);
@@ -832,7 +832,7 @@ int do_gauss(pbpic_handle* h, double* out) {
     CKLAUNCH("k_rho");
   }
   const pbpic_config& c = h->cfg;
-  k_gauss<T><<<grid_for(pe, 256), 256, 0, s>>>(c.mx, c.my, h->S, c.ybc, (const T*)h->f[0], (const T*)h->f[1],
+  k_gauss<T><<<grid_for(pe, 256), 256, 0, s>>>(c.mx, c.my, h->S, c.ybc, jlo, jhi, (const T*)h->f[0], (const T*)h->f[1],
                                                 h->rho, 1.0 / c.dx, 1.0 / c.dy, 1.0 / (c.cva * c.cva), c.in0,
                                                 h->dscalar);
   CKLAUNCH("k_gauss");
@@ -1235,7 +1235,14 @@ int pbpic_cell_counts(pbpic_handle* h, int32_t* counts) {
 int pbpic_gauss_residual(pbpic_handle* h, double* out) {
   TRY(check_handle(h));
   if (!out) return fail(PBPIC_EINVAL, "null argument");
-  return DISPATCH(h, do_gauss, h, out);
+  return DISPATCH(h, do_gauss, h, out, 0, h->cfg.my);
+}
+
+int pbpic_gauss_residual_rows(pbpic_handle* h, int32_t y_lo, int32_t y_hi, double* out) {
+  TRY(check_handle(h));
+  if (!out) return fail(PBPIC_EINVAL, "null argument");
+  if (y_lo < 0 || y_hi < y_lo || y_hi > h->cfg.my) return fail(PBPIC_EINVAL, "rows outside 0..my");
+  return DISPATCH(h, do_gauss, h, out, (int)y_lo, (int)y_hi);
 }
 
 int pbpic_reconnected_flux(pbpic_handle* h, double* out) {

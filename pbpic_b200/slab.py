@@ -24,7 +24,9 @@ refreshed every step:
   4. counting sort.
 The current needs no exchange: every particle that deposits into a slab's
 own rows is pushed on that slab (as an own particle or a ghost). Energies sum
-the own rows of every slab.
+the own rows of every slab and the Gauss residual takes the largest over the
+own rows, both reduced over the ranks by the transport (an all-reduce, as the
+reference's MPI_Allreduce of its energy sums, pic2d.f90:653-673).
 
 Transports: `InProcess` steps several slabs in one process (tests, or
 several domains on one GPU); `TorchDist` exchanges over torch.distributed
@@ -142,9 +144,18 @@ class GpuEngine:
         L.check(self.lib.pbpic_energies_rows(self.sim.handle, lo, hi, self.lay.wall_lo, self.lay.wall_hi, L.ptr(out)))
         return out
 
+    def gauss_residual(self):
+        v = ctypes.c_double()
+        L.check(self.lib.pbpic_gauss_residual_rows(self.sim.handle, self.lay.lo, self.lay.hi, ctypes.byref(v)))
+        return v.value
+
 
 class InProcess:
     """All slabs in this process; an exchange hands each band to its neighbour."""
+
+    def allreduce(self, values, op):
+        """Every slab is here: the process's own reduction is the whole one."""
+        return np.asarray(values, dtype=np.float64)
 
     def exchange(self, slabs, outgoing):
         """outgoing[r] = (to_down, to_up); returns incoming[r] = (from_down, from_up)."""
@@ -165,6 +176,13 @@ class TorchDist:
 
     def __init__(self, dist, device):
         self.dist, self.device = dist, device
+
+    def allreduce(self, values, op):
+        """values (float64) reduced over the ranks with op "sum" or "max"."""
+        import torch
+        t = torch.tensor(np.asarray(values, dtype=np.float64), device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM if op == "sum" else self.dist.ReduceOp.MAX)
+        return t.cpu().numpy()
 
     def _sendrecv(self, lay, sends, recvs):
         ops = []
@@ -248,6 +266,20 @@ class SlabRun:
                 e.set_field_rows(0, lay.gl, from_down)
             if from_up is not None:
                 e.set_field_rows(lay.hi, lay.gh, from_up)
+
+    def energies(self):
+        """Electron KE, ion KE, E and B energy of the whole domain (every rank
+        calls it: an all-reduce)."""
+        local = np.zeros(4)
+        for e in self.slabs.values():
+            local += e.energies()
+        return self.t.allreduce(local, "sum")
+
+    def gauss_residual(self):
+        """Largest Gauss's-law residual over the own rows of every slab (every
+        rank calls it: an all-reduce)."""
+        local = max(e.gauss_residual() for e in self.slabs.values())
+        return float(self.t.allreduce([local], "max")[0])
 
     def start(self):
         """Fill the ghost bands of freshly loaded slabs and sort."""

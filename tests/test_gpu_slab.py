@@ -2,7 +2,9 @@
 plasma: W slabs (W = 1, 2, 3, stepped in one process on one GPU, exchanging
 their ghost bands between steps) reproduce the single domain's particles
 (matched by id), fields and energies. FP64 plain: within 1e-12 relative (the
-order of the FP64 current sums differs); FP32 mixed: within FP32 rounding."""
+order of the FP64 current sums differs); FP32 mixed: within FP32 rounding. The
+slab run's energies and Gauss residual (reduced over the slabs) give the
+single domain's."""
 import numpy as np
 import pytest
 
@@ -46,7 +48,7 @@ def run_slabs(cfg, p0, f0, precision, world, steps):
     run = SlabRun(slabs, InProcess())
     run.start()
     run.step(steps)
-    return slabs
+    return slabs, run
 
 
 @pytest.mark.parametrize("world", [1, 2, 3])
@@ -56,7 +58,7 @@ def test_slabs_match_single_domain(gpu_lib, kind, world, precision):
     cfg, ld = global_case(kind)
     steps = 5
     single, p0, f0 = run_single(cfg, ld, precision, steps)
-    slabs = run_slabs(cfg, p0, f0, precision, world, steps)
+    slabs, run = run_slabs(cfg, p0, f0, precision, world, steps)
     ps = single.particles()
     n_own = 0
     for e in slabs.values():
@@ -98,3 +100,10 @@ def test_slabs_match_single_domain(gpu_lib, kind, world, precision):
     eg = sum(e.energies() for e in slabs.values())
     etol = 1e-11 if precision == "fp64" else 1e-5
     assert np.allclose(eg, es, rtol=etol, atol=etol * np.abs(es).max())
+    assert np.array_equal(run.energies(), eg)  # the slab run's reduction over its slabs
+    # Gauss's law over the own rows of every slab: the single domain's residual
+    gs, gg = single.gauss_residual(), run.gauss_residual()
+    if precision == "fp64":
+        assert abs(gg - gs) <= 1e-12
+    else:
+        assert max(gg, gs) <= 1e-5

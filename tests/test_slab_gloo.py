@@ -95,3 +95,48 @@ def test_two_slabs_over_gloo_match_single_oracle(oracle_mod, tmp_path, kind):
             fg[:, :, cfg["my"]] = np.load(tmp_path / f"top{r}.npy")
     rows = cfg["my"] + (1 if cfg["ybc"] == 1 else 0)
     assert np.abs(fg[:, :, :rows] - fs[:, :, :rows]).max() <= 1e-12 * np.abs(fs).max()
+
+
+class _FixedSlab:
+    """A slab whose own-row energies and Gauss residual are fixed numbers."""
+
+    def __init__(self, rank):
+        self.e = np.array([1.0, 2.0, 3.0, 4.0]) * (rank + 1)
+        self.g = 0.5 - 0.25 * rank
+
+    def energies(self):
+        return self.e
+
+    def gauss_residual(self):
+        return self.g
+
+
+def reduce_worker(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+
+    import torch.distributed as dist
+    from pbpic_b200.slab import SlabRun, TorchDist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    run = SlabRun({rank: _FixedSlab(rank)}, TorchDist(dist, "cpu"))
+    e = run.energies()
+    g = run.gauss_residual()
+    dist.destroy_process_group()
+    np.save(os.path.join(out_dir, f"red{rank}.npy"), np.concatenate([e, [g]]))
+
+
+def test_slab_energies_and_gauss_reduce_over_ranks(tmp_path):
+    """Every rank gets the sum of the slabs' energies and the largest of their
+    Gauss residuals (an all-reduce over gloo)."""
+    world = 3
+    port = free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=reduce_worker, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    for pr in procs:
+        pr.join(120)
+        assert pr.exitcode == 0
+    want = np.concatenate([np.array([1.0, 2.0, 3.0, 4.0]) * 6.0, [0.5]])
+    for r in range(world):
+        assert np.array_equal(np.load(tmp_path / f"red{r}.npy"), want)
