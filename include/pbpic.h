@@ -99,6 +99,13 @@ typedef struct pbpic_particle_f64 {
 #define PBPIC_LOAD_HARRIS 1     /* GEM Harris sheet along y with background, psi0 perturbation */
 #define PBPIC_LOAD_TWO_STREAM 2 /* counter-drifting electron beams along x */
 #define PBPIC_LOAD_WEIBEL 3     /* electrons with T_perp / T_par = anisotropy */
+/* The reference's own plasma (initparticles and initfields, pic2d.f90:357-648):
+ * two current sheets normal to x at Lx/4 and 3Lx/4 (half-thickness lambda) on a
+ * background nb, By = tanh((x - Lx/4)/lambda) - tanh((x - 3Lx/4)/lambda) - 1;
+ * sheet pairs drift along z at vdrift_i / vdrift_e in the first sheet and the
+ * opposite in the second, with thermal spread in x and y only (vthe, vthi);
+ * background pairs have vthe_bg, vthi_bg in x and y and no z motion. */
+#define PBPIC_LOAD_DOUBLE_HARRIS 4
 
 typedef struct pbpic_loader {
   int32_t kind;
@@ -115,6 +122,7 @@ typedef struct pbpic_loader {
   uint64_t seed;
   int32_t immobile_ions; /* nonzero: load electrons only (a fixed neutralising ion background) */
   int32_t reserved;
+  double vthe_bg, vthi_bg; /* double Harris: background thermal speeds / c */
 } pbpic_loader;
 
 typedef struct pbpic_handle pbpic_handle;

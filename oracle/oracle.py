@@ -32,7 +32,7 @@ class LoadParams(ctypes.Structure):  # pic::LoadParams in pbpic_b200/csrc/pic_co
                 ("npairs", ctypes.c_int64), ("nsheet", ctypes.c_int64), ("ppc", ctypes.c_int32),
                 ("uthe", ctypes.c_double), ("uthi", ctypes.c_double), ("uthe_perp", ctypes.c_double),
                 ("udrift_e", ctypes.c_double), ("udrift_i", ctypes.c_double), ("lambda_", ctypes.c_double),
-                ("seed", ctypes.c_uint64)]
+                ("seed", ctypes.c_uint64), ("uthe_bg", ctypes.c_double), ("uthi_bg", ctypes.c_double)]
 
 
 class FieldInit(ctypes.Structure):  # pic::FieldInit in pbpic_b200/csrc/pic_fields_init.h
@@ -193,9 +193,18 @@ def load_params(cfg, ld):
         ly = cfg["my"] * cfg["dy"]
         fs = 2.0 * ld["lambda_"] / (2.0 * ld["lambda_"] + ld["nb"] * ly)
         nsheet = int(round(npairs * fs))
+    if kind == 4:  # double Harris: an even number of sheet pairs, half in each sheet
+        lx = cfg["mx"] * cfg["dx"]
+        fs = 4.0 * ld["lambda_"] / (4.0 * ld["lambda_"] + ld["nb"] * lx)
+        nsheet = 2 * _round_half_away(0.5 * npairs * fs)
     return LoadParams(kind, cfg["mx"], cfg["my"], cfg["dx"], cfg["dy"], npairs, nsheet, ppc, uthe, uthi, uthe_perp,
                       u(ld.get("vdrift_e", 0.0)), u(ld.get("vdrift_i", 0.0)), ld.get("lambda_", 0.0),
-                      ld.get("seed", 0))
+                      ld.get("seed", 0), u(ld.get("vthe_bg", 0.0)), u(ld.get("vthi_bg", 0.0)))
+
+
+def _round_half_away(x):
+    """llround: halves away from zero (Python's round takes them to even)."""
+    return int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5))
 
 
 def load_plasma(cfg, ld):

@@ -3,7 +3,8 @@
 behind a C ABI (include/pbpic.h). This package is the Python view of that ABI.
 """
 from ._lib import (BC_CONDUCTING, BC_PERIODIC, COMPAT_BORIS, COMPAT_FOLD, COMPAT_RHO, FP32_MIXED, FP64_PLAIN,
-                   LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_UNIFORM, LOAD_WEIBEL, PARTICLE_F32, PARTICLE_F64,
+                   LOAD_DOUBLE_HARRIS, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_UNIFORM, LOAD_WEIBEL, PARTICLE_F32,
+                   PARTICLE_F64,
                    FILTER_CERENKOV, FILTER_MARDER, OPT_NO_AUTOSORT, STATUS_CELL_JUMP, STATUS_NAN, STATUS_UNSORTED,
                    PbpicError, lib)
 from .sim import Simulation, counting_sort_keys, kernel_launches
@@ -14,5 +15,5 @@ __all__ = [
     "BC_PERIODIC", "BC_CONDUCTING", "FP64_PLAIN", "FP32_MIXED",
     "COMPAT_BORIS", "COMPAT_FOLD", "COMPAT_RHO",
     "STATUS_CELL_JUMP", "STATUS_NAN", "STATUS_UNSORTED",
-    "LOAD_UNIFORM", "LOAD_HARRIS", "LOAD_TWO_STREAM", "LOAD_WEIBEL",
+    "LOAD_UNIFORM", "LOAD_HARRIS", "LOAD_TWO_STREAM", "LOAD_WEIBEL", "LOAD_DOUBLE_HARRIS",
 ]

@@ -18,7 +18,7 @@ BC_PERIODIC, BC_CONDUCTING = 0, 1
 FP64_PLAIN, FP32_MIXED = 0, 1
 COMPAT_BORIS, COMPAT_FOLD, COMPAT_RHO = 1, 2, 4
 STATUS_CELL_JUMP, STATUS_NAN, STATUS_UNSORTED = 1, 2, 4
-LOAD_UNIFORM, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_WEIBEL = 0, 1, 2, 3
+LOAD_UNIFORM, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_WEIBEL, LOAD_DOUBLE_HARRIS = 0, 1, 2, 3, 4
 FILTER_MARDER, FILTER_CERENKOV = 1, 2
 OPT_NO_AUTOSORT = 1
 
@@ -42,6 +42,7 @@ class Loader(ctypes.Structure):
         ("lambda_", ctypes.c_double), ("nb", ctypes.c_double), ("psi0", ctypes.c_double),
         ("bguide", ctypes.c_double), ("b0z", ctypes.c_double), ("anisotropy", ctypes.c_double),
         ("seed", ctypes.c_uint64), ("immobile_ions", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("vthe_bg", ctypes.c_double), ("vthi_bg", ctypes.c_double),
     ]
 
 

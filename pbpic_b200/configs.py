@@ -65,6 +65,29 @@ def harris(mx, my, ppc, seed, mime=25.0, wpe_wce=2.0, lam=0.5, nb=0.2, ti_te=5.0
     return cfg, ld
 
 
+def double_harris(mx=256, my=256, ppc=64, seed=5, dx=0.04, mime=25.0, cva=15.0, vthec=0.092, lam=0.5,
+                  ti_te=5.0, ti_te_bg=1.0, tbg_tcs=0.1, nb=0.2, bguide=0.0, dt=None):
+    """The reference's own run (module parameters, pic2d.f90:12-43; initparticles
+    and initfields, pic2d.f90:357-648): two current sheets normal to x at Lx/4
+    and 3Lx/4, half-thickness lam = 0.5 d_i, on a background nb = 0.2 n0, periodic
+    in x and y; 256x256 cells of 0.04 d_i, 64 particle pairs per cell, mi/me = 25,
+    c/v_A = 15, dt = 0.045/mime. Sheet electrons have thermal speed vthec c, sheet
+    ions Ti/Te = 5; the background is tbg_tcs times as hot, Ti/Te = 1; the sheets
+    drift at v_A (ions +z, electrons -z in the first sheet, the reverse in the
+    second). in0 = 1/(n0 dx dy) for the sheet peak density n0 (the formula the
+    reference keeps beside its hand-set value, pic2d.f90:31-33)."""
+    dy = dx
+    lx = mx * dx
+    vthe_bg = vthec * math.sqrt(tbg_tcs)
+    vd = 1.0 / cva
+    cfg = dict(mx=mx, my=my, dx=dx, dy=dy, dt=0.045 / mime if dt is None else dt, cva=cva, mime=mime,
+               in0=(4.0 * lam + nb * lx) / (ppc * lx), ybc=L.BC_PERIODIC)
+    ld = dict(kind=L.LOAD_DOUBLE_HARRIS, ppc=ppc, vthe=vthec, vthi=vthec * math.sqrt(ti_te / mime),
+              vthe_bg=vthe_bg, vthi_bg=vthe_bg * math.sqrt(ti_te_bg / mime), vdrift_e=-vd, vdrift_i=vd,
+              lambda_=lam, nb=nb, bguide=bguide, seed=seed)
+    return cfg, ld
+
+
 def harris_c2(seed=1, mx=1024, my=512, ppc=100):
     """GEM Harris sheet, 1024x512 cells of 0.1 d_i, 100 particles per cell per
     species (~105M), lambda = 0.5 d_i, nb = 0.2 n0, Ti/Te = 5, wpe/wce = 2,
@@ -149,4 +172,5 @@ WORKLOADS = {
     "harris_512x256_ppc100": harris_mid,
     "harris_256x128_ppc64": harris_c4,
     "harris_4096x2048_ppc100": harris_c5,
+    "double_harris_256x256_ppc64": double_harris,
 }

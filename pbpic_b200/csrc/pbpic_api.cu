@@ -755,6 +755,15 @@ pic::LoadParams loader_params(const pbpic_handle* h, const pbpic_loader* ld) {
   L.udrift_i = u(ld->vdrift_i);
   L.lambda = ld->lambda;
   L.seed = ld->seed;
+  L.uthe_bg = u(ld->vthe_bg);
+  L.uthi_bg = u(ld->vthi_bg);
+  if (ld->kind == PBPIC_LOAD_DOUBLE_HARRIS) {
+    // two sheets of 2 lambda n0 Ly particles each on nb n0 Lx Ly of background;
+    // an even count, one half per sheet (pic2d.f90:376-378)
+    const double Lx = c.mx * c.dx;
+    const double fs = 4.0 * ld->lambda / (4.0 * ld->lambda + ld->nb * Lx);
+    L.nsheet = 2 * (int64_t)llround(0.5 * (double)L.npairs * fs);
+  }
   if (ld->kind == PBPIC_LOAD_HARRIS) {
     const double Ly = c.my * c.dy;
     const double fs = 2.0 * ld->lambda / (2.0 * ld->lambda + ld->nb * Ly);
@@ -765,12 +774,14 @@ pic::LoadParams loader_params(const pbpic_handle* h, const pbpic_loader* ld) {
 
 int validate_loader(const pbpic_handle* h, const pbpic_loader* ld) {
   if (!ld) return fail(PBPIC_EINVAL, "null loader");
-  if (ld->kind < 0 || ld->kind > 3) return fail(PBPIC_EINVAL, "unknown loader kind");
+  if (ld->kind < 0 || ld->kind > 4) return fail(PBPIC_EINVAL, "unknown loader kind");
   if (ld->ppc <= 0) return fail(PBPIC_EINVAL, "loader ppc must be positive");
   if (ld->vthe < 0 || ld->vthe >= 1 || ld->vthi < 0 || ld->vthi >= 1) return fail(PBPIC_EINVAL, "thermal speeds must be in [0, c)");
   if (fabs(ld->vdrift_e) >= 1 || fabs(ld->vdrift_i) >= 1) return fail(PBPIC_EINVAL, "drift speeds must be below c");
-  if (ld->kind == PBPIC_LOAD_HARRIS && (ld->lambda <= 0 || ld->nb < 0))
+  if ((ld->kind == PBPIC_LOAD_HARRIS || ld->kind == PBPIC_LOAD_DOUBLE_HARRIS) && (ld->lambda <= 0 || ld->nb < 0))
     return fail(PBPIC_EINVAL, "Harris loader needs lambda > 0 and nb >= 0");
+  if (ld->kind == PBPIC_LOAD_DOUBLE_HARRIS && (ld->vthe_bg < 0 || ld->vthe_bg >= 1 || ld->vthi_bg < 0 || ld->vthi_bg >= 1))
+    return fail(PBPIC_EINVAL, "background thermal speeds must be in [0, c)");
   (void)h;
   return PBPIC_OK;
 }

@@ -205,6 +205,7 @@ enum LoadKind {
   LOAD_HARRIS = 1,      // GEM Harris sheet (normal along y) plus uniform background
   LOAD_TWO_STREAM = 2,  // counter-drifting electron beams along x
   LOAD_WEIBEL = 3,      // bi-Maxwellian electrons, T_perp / T_par = anisotropy
+  LOAD_DOUBLE_HARRIS = 4,  // two sheets normal to x at Lx/4, 3Lx/4 (pic2d.f90:357-578)
 };
 
 struct LoadParams {
@@ -219,6 +220,7 @@ struct LoadParams {
   double udrift_e, udrift_i;  // drift momenta (z for Harris, x for two-stream)
   double lambda;           // Harris half-thickness (d_i)
   uint64_t seed;
+  double uthe_bg, uthi_bg;  // double Harris: background thermal momenta (x and y)
 };
 
 // One loaded particle in double precision, before conversion to storage type.
@@ -257,6 +259,29 @@ PIC_HD void load_pair(const LoadParams& L, int64_t k, LoadedParticle out[2]) {
       pos.ox = PIC_DSUB(u01(r.v[0]), 0.5);
       pos.oy = PIC_DSUB(u01(r.v[1]), 0.5);
     } else {
+      place(L, PIC_DMUL(u01(r.v[0]), Lx), PIC_DMUL(u01(r.v[1]), Ly), &pos);
+    }
+  } else if (L.kind == LOAD_DOUBLE_HARRIS) {
+    if (k < L.nsheet) {
+      // even pairs in the sheet at Lx/4, odd ones in the sheet at 3Lx/4; x from
+      // the sech^2 profile by the logistic sampling of pic2d.f90:398-412 and
+      // 453-466, redrawn outside the box; y uniform
+      const double xc = PIC_DMUL((k & 1) ? 0.75 : 0.25, Lx);
+      double x = xc, y = 0.0;
+      for (uint64_t attempt = 0; attempt < 1024; ++attempt) {
+        u64x4 r = philox4x64((uint64_t)k, 0, attempt, 0, key0, key1);
+        double u = u01(r.v[0]);
+        if (u < 1e-10) u = 1e-10;
+        if (u > 1.0 - 1e-10) u = 1.0 - 1e-10;
+        double t = pic_log(PIC_DDIV(u, PIC_DSUB(1.0, u)));
+        x = PIC_DADD(xc, PIC_DMUL(PIC_DMUL(0.5, L.lambda), t));
+        y = PIC_DMUL(u01(r.v[1]), Ly);
+        if (x >= 0.0 && x < Lx) break;
+        x = xc;
+      }
+      place(L, x, y, &pos);
+    } else {
+      u64x4 r = philox4x64((uint64_t)k, 0, 0, 0, key0, key1);
       place(L, PIC_DMUL(u01(r.v[0]), Lx), PIC_DMUL(u01(r.v[1]), Ly), &pos);
     }
   } else {  // LOAD_HARRIS
@@ -298,6 +323,18 @@ PIC_HD void load_pair(const LoadParams& L, int64_t k, LoadedParticle out[2]) {
       out[1].ux = PIC_DMUL(ge0, L.uthe);
       out[1].uy = PIC_DMUL(ge1, L.uthe);
       out[1].uz = PIC_DADD(PIC_DMUL(ge2, L.uthe), sheet ? L.udrift_e : 0.0);
+      break;
+    }
+    case LOAD_DOUBLE_HARRIS: {  // pic2d.f90:436-448, 490-502, 539-551: no thermal motion along z
+      const bool sheet = k < L.nsheet;
+      const double sgn = (k & 1) ? -1.0 : 1.0;  // the second sheet drifts the other way
+      const double ui = sheet ? L.uthi : L.uthi_bg, ue = sheet ? L.uthe : L.uthe_bg;
+      out[0].ux = PIC_DMUL(gi0, ui);
+      out[0].uy = PIC_DMUL(gi1, ui);
+      out[0].uz = sheet ? PIC_DMUL(sgn, L.udrift_i) : 0.0;
+      out[1].ux = PIC_DMUL(ge0, ue);
+      out[1].uy = PIC_DMUL(ge1, ue);
+      out[1].uz = sheet ? PIC_DMUL(sgn, L.udrift_e) : 0.0;
       break;
     }
     case LOAD_TWO_STREAM: {

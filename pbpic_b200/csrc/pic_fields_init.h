@@ -38,8 +38,13 @@ inline double init_bx(const FieldInit& f, int i, int j) {
   return b - dpsi / f.dy;
 }
 
-// By at (i, j+1/2).
+// By at (i, j+1/2). Double Harris (kind 4): the two sheets' profile at the node
+// column x = i dx (initfields, pic2d.f90:606-610).
 inline double init_by(const FieldInit& f, int i, int j) {
+  if (f.kind == 4) {
+    const double Lx = f.mx * f.dx, x = i * f.dx;
+    return tanh((x - 0.25 * Lx) / f.lambda) - tanh((x - 0.75 * Lx) / f.lambda) - 1.0;
+  }
   if (f.kind != 1) return 0.0;
   double yc = (j + 0.5) * f.dy;
   double dpsi = gem_psi(f, (i + 0.5) * f.dx, yc) - gem_psi(f, (i - 0.5) * f.dx, yc);
@@ -48,7 +53,7 @@ inline double init_by(const FieldInit& f, int i, int j) {
 
 // Bz at (i+1/2, j+1/2).
 inline double init_bz(const FieldInit& f, int /*i*/, int /*j*/) {
-  if (f.kind == 1) return f.bguide;
+  if (f.kind == 1 || f.kind == 4) return f.bguide;
   return f.b0z;
 }
 

@@ -21,6 +21,9 @@ def plasma(O, ybc, mx=16, my=12, ppc=8, seed=5, vthe=0.3, kind="uniform"):
     if kind == "harris":
         cfg, ld = configs.harris(mx, my, ppc, seed=seed)
         cfg["ybc"] = ybc
+    elif kind == "double_harris":
+        cfg, ld = configs.double_harris(mx, my, ppc, seed=seed)
+        cfg["ybc"] = ybc
     else:
         cfg, ld = configs.uniform_c1(mx=mx, my=my, ppc=ppc, seed=seed)
         cfg["ybc"] = ybc
@@ -151,7 +154,8 @@ def test_mixed_is_bit_reproducible(gpu_lib):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_device_loader_matches_cpu_loader(gpu_lib, oracle_mod, precision):
-    for cfg, ld in (configs.uniform_c1(mx=16, my=8, ppc=8, seed=2), configs.harris(32, 16, 8, seed=6)):
+    for cfg, ld in (configs.uniform_c1(mx=16, my=8, ppc=8, seed=2), configs.harris(32, 16, 8, seed=6),
+                    configs.double_harris(64, 16, 8, seed=9)):
         p, yee = oracle_mod.load_plasma(cfg, ld)
         ref = p[np.argsort(p["grid"], kind="stable")]
         with new_sim(cfg, len(p), precision=precision) as s:
@@ -167,7 +171,7 @@ def test_device_loader_matches_cpu_loader(gpu_lib, oracle_mod, precision):
             assert np.array_equal(f[:, :, :rows], want[:, :, :rows])
 
 
-@pytest.mark.parametrize("ybc,kind", [(0, "uniform"), (1, "harris")])
+@pytest.mark.parametrize("ybc,kind", [(0, "uniform"), (1, "harris"), (0, "double_harris")])
 def test_plain_energy_history_matches_oracle(gpu_lib, oracle_mod, ybc, kind):
     cfg, ld, p, yee = plasma(oracle_mod, ybc, mx=32, my=16, ppc=8, kind=kind)
     o = oracle_mod.Oracle(**cfg)

@@ -251,3 +251,44 @@ def test_field_filters_match_numpy(oracle_mod, flags):
         if c < 2 or flags & 2:
             assert np.abs(want[c]).max() > 1e-6
 
+
+
+def test_double_harris_loader(oracle_mod):
+    """The reference's own plasma (pic2d.f90:357-648): co-located pairs, an even
+    number of sheet pairs alternating between the sheets at Lx/4 and 3Lx/4 with
+    a sech^2 profile in x (mean |x - xc| = lambda ln 2), drifts of opposite sign
+    in the two sheets and none in the background, no thermal motion along z,
+    and By = tanh((x - Lx/4)/lambda) - tanh((x - 3Lx/4)/lambda) - 1 on the node
+    columns with every other field component zero."""
+    from pbpic_b200 import configs
+    cfg, ld = configs.double_harris(mx=256, my=8, ppc=8, seed=11)
+    p, yee = oracle_mod.load_plasma(cfg, ld)
+    lp = oracle_mod.load_params(cfg, ld)
+    mx, my, dx, lam = cfg["mx"], cfg["my"], cfg["dx"], ld["lambda_"]
+    lx = mx * dx
+    npairs = ld["ppc"] * mx * my
+    assert len(p) == 2 * npairs and lp.nsheet % 2 == 0
+    assert abs(lp.nsheet - npairs * 4 * lam / (4 * lam + ld["nb"] * lx)) <= 1.0
+    ion, ele = p[0::2], p[1::2]
+    assert np.all(ion["q"] == 1) and np.all(ele["q"] == -1)
+    for c in ("grid", "dx", "dy"):
+        assert np.array_equal(ion[c], ele[c])  # zero initial charge density
+    ix = (ion["grid"] - 1) // my
+    x = (ix + 0.5 + ion["dx"]) * dx
+    k = np.arange(npairs)
+    sheet = k < lp.nsheet
+    for parity, xc in ((0, 0.25 * lx), (1, 0.75 * lx)):
+        m = sheet & (k % 2 == parity)
+        assert abs(np.mean(np.abs(x[m] - xc)) - lam * math.log(2.0)) < 0.02
+        sgn = 1.0 if parity == 0 else -1.0
+        assert np.allclose(ion["uz"][m], sgn * lp.udrift_i, rtol=0, atol=1e-15)
+        assert np.allclose(ele["uz"][m], sgn * lp.udrift_e, rtol=0, atol=1e-15)
+    assert lp.udrift_i > 0 > lp.udrift_e
+    assert np.all(ion["uz"][~sheet] == 0) and np.all(ele["uz"][~sheet] == 0)
+    # thermal spread in x and y: sheet and background temperatures
+    assert abs(np.std(ele["ux"][sheet]) / lp.uthe - 1) < 0.05
+    assert abs(np.std(ion["uy"][~sheet]) / lp.uthi_bg - 1) < 0.05
+    xs = np.arange(mx) * dx
+    by = np.tanh((xs - 0.25 * lx) / lam) - np.tanh((xs - 0.75 * lx) / lam) - 1.0
+    assert np.allclose(yee[4], by[:, None], rtol=0, atol=1e-15)
+    assert not yee[[0, 1, 2, 3, 5]].any()
