@@ -12,8 +12,10 @@
 //     every ntdiag steps: energyinfo -> pbpic_energies            (pic2d.f90:183-187)
 //   releasememory            -> pbpic_destroy                     (pic2d.f90:189, 2557-2582)
 //
-// Usage: pic2d_driver [--harris|--uniform] [--mx N] [--my N] [--ppc N] [--ntime N]
-//                     [--sort-every N] [--ntdiag N] [--fp32|--fp64] [--seed N]
+// Usage: pic2d_driver [--double-harris|--harris|--uniform] [--mx N] [--my N] [--ppc N]
+//                     [--ntime N] [--sort-every N] [--ntdiag N] [--fp32|--fp64] [--seed N]
+// The default is the reference's own run: its double Harris sheet on 256x256
+// cells of 0.04 d_i, 64 pairs per cell, 30 steps (pic2d.f90:12-43, 357-648).
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -23,9 +25,11 @@
 
 namespace {
 
+enum Plasma { DOUBLE_HARRIS, HARRIS, UNIFORM };
+
 struct Parameters {  // the run parameters of module parameters (pic2d.f90:12-43, 127-136)
-  int mx = 256, my = 128, ppc = 64, ntime = 30, sort_every = 50, ntdiag = 10;
-  int harris = 1, precision = PBPIC_FP32_MIXED;
+  int mx = 256, my = 256, ppc = 64, ntime = 30, sort_every = 50, ntdiag = 10;
+  int plasma = DOUBLE_HARRIS, precision = PBPIC_FP32_MIXED;
   double mime = 25.0, wpe_wce = 2.0;
   unsigned long long seed = 1;
 };
@@ -59,7 +63,28 @@ void init() {
   cfg.cva = cva;
   cfg.mime = prm.mime;
   cfg.precision = prm.precision;
-  if (prm.harris) {
+  if (prm.plasma == DOUBLE_HARRIS) {
+    // the reference's parameters (pic2d.f90:15-31, 42): dx = 0.04 d_i, c/v_A = 15,
+    // dt = 0.045 / mime, sheet electrons at 0.092 c with Ti/Te = 5, the background
+    // 10 times colder with Ti/Te = 1 and nb = 0.2, sheets of half-width 0.5 d_i
+    // drifting at v_A
+    const double ddx = 0.04, c_va = 15.0, vthec = 0.092, lam = 0.5, nb = 0.2;
+    cfg.dx = cfg.dy = ddx;
+    cfg.cva = c_va;
+    cfg.dt = 0.045 / prm.mime;
+    ld.kind = PBPIC_LOAD_DOUBLE_HARRIS;
+    ld.vthe = vthec;
+    ld.vthi = vthec * sqrt(5.0 / prm.mime);
+    ld.vthe_bg = vthec * sqrt(0.1);
+    ld.vthi_bg = ld.vthe_bg * sqrt(1.0 / prm.mime);
+    ld.vdrift_i = 1.0 / c_va;
+    ld.vdrift_e = -1.0 / c_va;
+    ld.lambda = lam;
+    ld.nb = nb;
+    cfg.ybc = PBPIC_BC_PERIODIC;
+    const double lx = prm.mx * ddx;
+    cfg.in0 = (4.0 * lam + nb * lx) / (prm.ppc * lx);  // 1 / (n0 dx dy), n0 the sheet peak density
+  } else if (prm.plasma == HARRIS) {
     // Harris sheet in pressure balance, Ti/Te = 5, lambda = 0.5 d_i, nb = 0.2 n0
     const double tite = 5.0, lam = 0.5, nb = 0.2;
     const double te = 1.0 / (2.0 * (1.0 + tite));
@@ -110,8 +135,9 @@ void parse(int argc, char** argv) {
       }
       return argv[++i];
     };
-    if (!strcmp(argv[i], "--harris")) prm.harris = 1;
-    else if (!strcmp(argv[i], "--uniform")) prm.harris = 0;
+    if (!strcmp(argv[i], "--double-harris")) prm.plasma = DOUBLE_HARRIS;
+    else if (!strcmp(argv[i], "--harris")) prm.plasma = HARRIS;
+    else if (!strcmp(argv[i], "--uniform")) prm.plasma = UNIFORM;
     else if (!strcmp(argv[i], "--mx")) prm.mx = atoi(next());
     else if (!strcmp(argv[i], "--my")) prm.my = atoi(next());
     else if (!strcmp(argv[i], "--ppc")) prm.ppc = atoi(next());

@@ -12,7 +12,9 @@ DRIVER = os.path.join(ROOT, "pbpic_b200", "pic2d_driver")
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("args", [["--uniform", "--mx", "32", "--my", "32", "--ppc", "8", "--fp64"],
-                                  ["--harris", "--mx", "64", "--my", "32", "--ppc", "16", "--fp32"]])
+                                  ["--harris", "--mx", "64", "--my", "32", "--ppc", "16", "--fp32"],
+                                  ["--double-harris", "--mx", "256", "--my", "16", "--ppc", "16", "--fp64"],
+                                  []])  # the reference's own run: double Harris, 256x256, 64 pairs per cell
 def test_driver_time_loop(gpu_lib, args):
     r = subprocess.run([DRIVER, *args, "--ntime", "30", "--ntdiag", "10", "--sort-every", "5"],
                        capture_output=True, text=True, timeout=300)
