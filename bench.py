@@ -325,13 +325,14 @@ def run_cpu_sample(workload_name, steps, seed_offset=0):
 
 
 def run_cpu_single_f32(steps=3):
-    """One host thread of the oracle in FP32 (the reference's own precision)
-    on the 128x128 uniform plasma, 32 particles per cell per species."""
+    """One host thread of the oracle in FP32 with every compat switch on (the
+    reference's own precision and arithmetic) on the 128x128 uniform plasma,
+    32 particles per cell per species."""
     from oracle import oracle as O
     from pbpic_b200 import configs
     cfg, ld = configs.uniform_c1()
     p, yee = O.load_plasma(cfg, ld)
-    o = O.Oracle(**cfg, precision="f32")
+    o = O.Oracle(**dict(cfg, compat=7), precision="f32")
     o.load_particles(p)
     del p
     o.set_fields(yee)
@@ -345,8 +346,8 @@ def run_cpu_single_f32(steps=3):
     n = o.L.orc_nptl(o.h)
     o.close()
     return {"value": n * steps / dt, "unit": UNIT, "cores": 1,
-            "sample": f"{cfg['mx']}x{cfg['my']} cells, {n} particles, {steps} steps of push+fieldsolve+sort, FP32, "
-                      "one thread"}
+            "sample": f"{cfg['mx']}x{cfg['my']} cells, {n} particles, {steps} steps of push+fieldsolve+sort, FP32 with "
+                      "the compat switches (7), one thread"}
 
 
 def main():
