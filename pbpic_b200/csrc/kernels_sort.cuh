@@ -443,7 +443,10 @@ struct ScatterSmem {
 // perm[d] = p. The particle data stay where they are; the next push reads
 // them through perm (PushParams::src), and a gather (k_gather) applies perm
 // when the arrays themselves must be in cell order.
-constexpr int SP_IPT = 8, SP_CHUNK = 256 * SP_IPT;
+#ifndef PBPIC_PERM_IPT
+#define PBPIC_PERM_IPT 8  // particles per thread in one chunk of the ranking
+#endif
+constexpr int SP_IPT = PBPIC_PERM_IPT, SP_CHUNK = 256 * SP_IPT;
 
 template <class T>
 __device__ __forceinline__ void perm_tile(const ScatterParams<T>& a, const int t, ScatterSmem& sm) {
