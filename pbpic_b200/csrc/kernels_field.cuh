@@ -27,6 +27,7 @@ struct FieldParams {
   const void* jacc;      // 4 planes of accumulators (double or int64)
   double jscale[4];      // accumulator -> normalised current (in0, fixed-point scale)
   T* ng;                 // node grid (mx+1) x (my+1) x 8
+  T* cg;                 // mixed form: per-cell gather records mx x my x 24 of the push
   double* fe_part;       // per-block field energy partial sums [grid][2]
   int nblk;              // batched launches: blocks that compute the partials
 };
@@ -194,6 +195,30 @@ __global__ void k_nodes(FieldParams<T> a) {
   nodes_body(a, red, blockIdx.x, gridDim.x);
 }
 
+// Gather records of the mixed-form push from the node grid: cell (cx, cy) gets
+// its nodes (cx, cy), (cx, cy+1), (cx+1, cy), (cx+1, cy+1), each ex ey ez bx by
+// bz, as 6 contiguous 16-byte stores, so the push reads a cell's 4 nodes with 6
+// loads from one address instead of 8 from two.
+__device__ __forceinline__ void cell_records_body(const FieldParams<float>& a, int bid, int nblk) {
+  const long long n = (long long)a.mx * a.my;
+  for (long long c = bid * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)nblk * blockDim.x) {
+    const int cx = (int)(c / a.my), cy = (int)(c - (long long)cx * a.my);
+    const float4* g00 = reinterpret_cast<const float4*>(a.ng + ((long long)cx * (a.my + 1) + cy) * 8);
+    const float4* g10 = g00 + 2 * (long long)(a.my + 1);
+    const float4 p0 = g00[0], q0 = g00[1], p1 = g00[2], q1 = g00[3];  // nodes 00, 01: ex ey ez 0 | bx by bz 0
+    const float4 p2 = g10[0], q2 = g10[1], p3 = g10[2], q3 = g10[3];  // nodes 10, 11
+    float4* r = reinterpret_cast<float4*>(a.cg + c * 24);
+    r[0] = make_float4(p0.x, p0.y, p0.z, q0.x);
+    r[1] = make_float4(q0.y, q0.z, p1.x, p1.y);
+    r[2] = make_float4(p1.z, q1.x, q1.y, q1.z);
+    r[3] = make_float4(p2.x, p2.y, p2.z, q2.x);
+    r[4] = make_float4(q2.y, q2.z, p3.x, p3.y);
+    r[5] = make_float4(p3.z, q3.x, q3.y, q3.z);
+  }
+}
+
+static __global__ void k_cell_records(FieldParams<float> a) { cell_records_body(a, blockIdx.x, gridDim.x); }
+
 // Optional field filters, periodic y only: Marder divergence cleaning
 // (divergenceclean, pic2d.f90:867-886) and the Cherenkov filter
 // (suppresscerenkov, pic2d.f90:889-907), whose call the reference comments
@@ -293,6 +318,12 @@ __global__ void k_nodes_batched(const FieldParams<T>* d) {
   if (threadIdx.x == 0) a = d[blockIdx.y];
   __syncthreads();
   if ((int)blockIdx.x < a.nblk) nodes_body(a, red, blockIdx.x, a.nblk);
+}
+static __global__ void k_cell_records_batched(const FieldParams<float>* d) {
+  __shared__ FieldParams<float> a;
+  if (threadIdx.x == 0) a = d[blockIdx.y];
+  __syncthreads();
+  cell_records_body(a, blockIdx.x, gridDim.x);
 }
 
 // Sum the per-tile kinetic and per-block field partials in a fixed order and

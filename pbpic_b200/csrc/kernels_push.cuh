@@ -59,6 +59,7 @@ struct PushParams {
   uint32_t* cell;
   T *dx, *dy, *ux, *uy, *uz;
   const T* ng;      // node fields (mx+1) x (my+1) x 8: ex ey ez 0 bx by bz 0
+  const T* cg;      // mixed form: per-cell gather records mx x my x 24 (k_cell_records)
   void* jacc;       // 4 planes (jx, jy, jz, rho) of mx x S accumulators
   int32_t* tilecnt; // [ntiles][3*(tile_rows+2)] new-cell counts (HIST)
   const int32_t* cell_off;  // [mx*my + 1] cell offsets of the sorted input (HIST)
@@ -89,6 +90,18 @@ __device__ __forceinline__ Node6<double> load_node(const double* g) {
   const double2* p = reinterpret_cast<const double2*>(g);
   double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
   return Node6<double>{a.x, a.y, b.x, c.x, c.y, d.x};
+}
+
+// The 4 gather nodes of a cell from its record: n00, n01, n10, n11, each ex ey
+// ez bx by bz (6 aligned 16-byte loads from one address).
+__device__ __forceinline__ void load_cell(const float* r, Node6<float>& n00, Node6<float>& n01, Node6<float>& n10,
+                                          Node6<float>& n11) {
+  const float4* q = reinterpret_cast<const float4*>(r);
+  const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4), f = __ldg(q + 5);
+  n00 = Node6<float>{a.x, a.y, a.z, a.w, b.x, b.y};
+  n01 = Node6<float>{b.z, b.w, c.x, c.y, c.z, c.w};
+  n10 = Node6<float>{d.x, d.y, d.z, d.w, e.x, e.y};
+  n11 = Node6<float>{e.z, e.w, f.x, f.y, f.z, f.w};
 }
 
 __device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
@@ -657,12 +670,16 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
         const int cid = (ix << 16) | iy;
         if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
-          const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
-          const T* g10 = g00 + (long long)(a.my + 1) * 8;
-          n00 = load_node(g00);
-          n01 = load_node(g00 + 8);
-          n10 = load_node(g10);
-          n11 = load_node(g10 + 8);
+          if constexpr (MIXED) {
+            load_cell(a.cg + ((long long)ix * a.my + iy) * 24, n00, n01, n10, n11);
+          } else {  // FP64: from the node grid (its records took more registers than they saved)
+            const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
+            const T* g10 = g00 + (long long)(a.my + 1) * 8;
+            n00 = load_node(g00);
+            n01 = load_node(g00 + 8);
+            n10 = load_node(g10);
+            n11 = load_node(g10 + 8);
+          }
           cache_cell = cid;
         }
         Pushed<T> o;

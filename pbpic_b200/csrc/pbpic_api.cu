@@ -147,6 +147,7 @@ struct pbpic_handle {
   int cur = 0;
   void* f[6] = {nullptr};
   void* ng = nullptr;
+  void* cg = nullptr;  // mixed form: per-cell gather records of the push (k_cell_records after k_nodes)
   void* jacc = nullptr;
   int32_t *counts = nullptr, *off = nullptr, *tile_off = nullptr;
   double *ke_part = nullptr, *fe_part = nullptr;
@@ -296,6 +297,7 @@ PushParams<T> push_params(pbpic_handle* h) {
   p.uy = P<T>(h, b, 3);
   p.uz = P<T>(h, b, 4);
   p.ng = (const T*)h->ng;
+  p.cg = (const T*)h->cg;
   p.jacc = h->jacc;
   p.tilecnt = h->tilecnt;
   p.cell_off = h->off;
@@ -354,6 +356,7 @@ FieldParams<T> field_params(pbpic_handle* h) {
     for (int k = 0; k < 4; ++k) a.jscale[k] = c.in0;
   }
   a.ng = (T*)h->ng;
+  a.cg = (T*)h->cg;
   a.fe_part = h->fe_part;
   return a;
 }
@@ -368,6 +371,10 @@ int nodes_and_field_energy(pbpic_handle* h, int row) {
   FieldParams<T> a = field_params<T, MIXED>(h);
   k_nodes<T><<<h->nfe, 256, 0, h->stream>>>(a);
   CKLAUNCH("k_nodes");
+  if constexpr (MIXED) {
+    k_cell_records<<<h->nfe, 256, 0, h->stream>>>(a);
+    CKLAUNCH("k_cell_records");
+  }
   k_energy_row<<<1, 256, 0, h->stream>>>(nullptr, 0, h->fe_part, h->nfe, fe_scale(h->cfg), fb_scale(h->cfg),
                                           h->hist + (size_t)row * 4);
   CKLAUNCH("k_energy_row");
@@ -493,6 +500,7 @@ int do_push(pbpic_handle* h) {
   TRY((push_smem_optin<T, MIXED>(h)));
   const bool hist = h->sorted && h->fused_ok;
   if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
+  if (MIXED && !p.cg) return fail(PBPIC_ESTATE, "k_push: no per-cell gather records");
   const int nt = PushThreads<T>::value;
   const bool compat = h->cfg.compat != 0;
   if (h->lazy) {  // read through the sort's permutation, write in cell order to the other buffer
@@ -937,6 +945,7 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
   }
   for (int k = 0; k < 6; ++k) A(&h->f[k], (size_t)pe * h->tsz);
   A(&h->ng, (size_t)(c.mx + 1) * (c.my + 1) * 8 * h->tsz);
+  if (h->mixed) A(&h->cg, (size_t)c.mx * c.my * 24 * h->tsz);
   A(&h->jacc, (size_t)4 * pe * 8);
   A(&h->counts, (size_t)(h->ncells + 1) * 4);
   A(&h->off, (size_t)(h->ncells + 1) * 4);
@@ -961,6 +970,7 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
   }
   for (int k = 0; k < 6; ++k) cudaMemset(h->f[k], 0, (size_t)pe * h->tsz);
   cudaMemset(h->ng, 0, (size_t)(c.mx + 1) * (c.my + 1) * 8 * h->tsz);
+  if (h->cg) cudaMemset(h->cg, 0, (size_t)c.mx * c.my * 24 * h->tsz);
   cudaMemset(h->jacc, 0, (size_t)4 * pe * 8);
   cudaMemset(h->counts, 0, (size_t)(h->ncells + 1) * 4);
   cudaMemset(h->off, 0, (size_t)(h->ncells + 1) * 4);
@@ -1422,7 +1432,7 @@ extern "C" int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t 
 //   k_fused_counts_batched, k_scan_batched, k_fused_base_batched,
 //   k_fused_perm_batched (persistent), k_tile_off_batched
 //                          the fused counting sort of every domain
-//   k_bhalf/k_efull/k_bhalf/k_nodes_batched, k_energy_rows_batched
+//   k_bhalf/k_efull/k_bhalf/k_nodes_batched, k_cell_records_batched, k_energy_rows_batched
 // Two consecutive steps (the particle buffers swap each step) are captured
 // once in a CUDA graph and replayed. A domain stepped here goes through the
 // same arithmetic as pbpic_step(h, n, 1) with the same tile rows and
@@ -1720,6 +1730,8 @@ int batch_enqueue_step(pbpic_batch* b, int par) {
   CKLAUNCH("k_bhalf_batched");
   k_nodes_batched<float><<<dim3(b->gx_nodes, D), 256, 0, s>>>(b->d_field);
   CKLAUNCH("k_nodes_batched");
+  k_cell_records_batched<<<dim3(b->gx_nodes, D), 256, 0, s>>>(b->d_field);
+  CKLAUNCH("k_cell_records_batched");
   k_energy_rows_batched<<<D, 256, 0, s>>>(b->d_erow, ctr + 2);
   CKLAUNCH("k_energy_rows_batched");
   return PBPIC_OK;

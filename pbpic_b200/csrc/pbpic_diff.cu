@@ -145,6 +145,7 @@ PushParams<T> push_params(const pbpic_diff* d, const Slot& s) {
   p.uy = v.c[3];
   p.uz = v.c[4];
   p.ng = (const T*)d->ng;
+  p.cg = nullptr;  // the adjoint kernels gather from the node grid
   p.jacc = d->jacc;
   const T dt = (T)d->dt, mime = (T)d->cfg.mime, cva = (T)d->cva, dx = (T)d->dx, dy = (T)d->dy;
   for (int sp = 0; sp < 2; ++sp) {
@@ -186,6 +187,7 @@ FieldParams<T> field_params(const pbpic_diff* d, const Slot& s) {
   a.jacc = d->jacc;
   for (int k = 0; k < 4; ++k) a.jscale[k] = d->f32 ? d->in0 * FIX_INV : d->in0;
   a.ng = (T*)d->ng;
+  a.cg = nullptr;
   a.fe_part = d->fe_part;
   return a;
 }

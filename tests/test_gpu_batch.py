@@ -132,4 +132,4 @@ def test_batch_counts_graph_launches(gpu_lib):
         n0 = kernel_launches()
         b.step(4)
         b.synchronize()
-        assert kernel_launches() - n0 == 4 * 12  # 12 kernels per batched step
+        assert kernel_launches() - n0 == 4 * 13  # 13 kernels per batched step
