@@ -81,6 +81,25 @@ class OracleEngine:
         q["grid"] = (ix[m] * self.lay.my + iy[m] - self.lay.gl + self.lay.y0 + 1).astype(np.int32)
         return q
 
+    def energies(self):
+        """Electron KE, ion KE, E and B energy of the own rows, summed as the
+        oracle sums them (kinetic energy pic2d.f90:1055-1062 from the particles'
+        momenta, fieldsenergy pic2d.f90:653-673 over the own node rows with the
+        trapezoid weight 1/2 on global wall rows)."""
+        q = self.own_particles()
+        gm1 = np.sqrt(1.0 + q["ux"] ** 2 + q["uy"] ** 2 + q["uz"] ** 2) - 1.0
+        mime, cva2, in0 = self.cfg["mime"], self.cfg["cva"] ** 2, self.cfg["in0"]
+        lo, hi = self.lay.energy_rows()
+        g = self.o.emfgrid()[:self.mx, lo:hi]
+        w = np.ones(hi - lo)
+        for r in (self.lay.wall_lo, self.lay.wall_hi):
+            if r >= 0 and lo <= r < hi:
+                w[r - lo] = 0.5
+        se = float(((g[..., 0] ** 2 + g[..., 1] ** 2 + g[..., 2] ** 2) * w).sum())
+        sb = float(((g[..., 4] ** 2 + g[..., 5] ** 2 + g[..., 6] ** 2) * w).sum())
+        return np.array([gm1[q["q"] == -1].sum(), mime * gm1[q["q"] == 1].sum(),
+                         0.5 * se * mime / (cva2 * cva2 * in0), 0.5 * sb * mime / (cva2 * in0)])
+
     def own_fields(self):
         f = self.o.fields()
         out = f[:, :, self.lay.lo:self.lay.hi]

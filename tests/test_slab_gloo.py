@@ -2,7 +2,8 @@
 point-to-point exchanges of the ghost bands, sizes then payloads), each rank
 stepping its slab with the CPU oracle: the own particles and field rows of
 the two ranks reproduce the single-domain oracle run within 1e-12 relative
-(FP64; the order of the current sums differs), periodic and conducting y."""
+(FP64; the order of the current sums differs), periodic and conducting y, and
+every rank's all-reduced energies are the single domain's."""
 import json
 import multiprocessing as mp
 import os
@@ -49,7 +50,9 @@ def worker(rank, world, port, kind, steps, out_dir):
     run.step(steps)
     q = e.own_particles()
     f, top = e.own_fields()
+    en = run.energies()  # every rank: an all-reduce of the slabs' own-row energies
     dist.destroy_process_group()
+    np.save(os.path.join(out_dir, f"e{rank}.npy"), en)
     np.save(os.path.join(out_dir, f"p{rank}.npy"), q)
     np.save(os.path.join(out_dir, f"f{rank}.npy"), f)
     if top is not None:
@@ -95,6 +98,9 @@ def test_two_slabs_over_gloo_match_single_oracle(oracle_mod, tmp_path, kind):
             fg[:, :, cfg["my"]] = np.load(tmp_path / f"top{r}.npy")
     rows = cfg["my"] + (1 if cfg["ybc"] == 1 else 0)
     assert np.abs(fg[:, :, :rows] - fs[:, :, :rows]).max() <= 1e-12 * np.abs(fs).max()
+    es = o.energies()  # the single domain's totene row of its last step
+    for r in range(world):
+        assert np.allclose(np.load(tmp_path / f"e{r}.npy"), es, rtol=1e-10, atol=1e-14 * np.abs(es).max())
 
 
 class _FixedSlab:
