@@ -15,7 +15,10 @@
 ! ptl(1:nptlact) into an array of c_particle before loading.
 !
 ! Not compiled in the build environment of this repository (it has no Fortran
-! compiler); the interfaces follow include/pbpic.h one to one.
+! compiler). It declares every single-handle function of include/pbpic.h that
+! a Fortran time loop uses, with the header's argument order and types; the
+! batched, differentiable and slab-band entry points (C and Python callers)
+! are left out.
 !******************************************************************************
 module pbpic_gpu
     use iso_c_binding
@@ -27,6 +30,8 @@ module pbpic_gpu
     integer(c_int32_t), parameter :: PBPIC_COMPAT_BORIS = 1, PBPIC_COMPAT_FOLD = 2, PBPIC_COMPAT_RHO = 4
     integer(c_int32_t), parameter :: PBPIC_OPT_NO_AUTOSORT = 1
     integer(c_int32_t), parameter :: PBPIC_FILTER_MARDER = 1, PBPIC_FILTER_CERENKOV = 2
+    integer(c_int32_t), parameter :: PBPIC_LOAD_UNIFORM = 0, PBPIC_LOAD_HARRIS = 1, PBPIC_LOAD_TWO_STREAM = 2, &
+                                     PBPIC_LOAD_WEIBEL = 3, PBPIC_LOAD_DOUBLE_HARRIS = 4
 
     type, bind(c) :: pbpic_config
         integer(c_int32_t) :: mx, my
@@ -39,6 +44,22 @@ module pbpic_gpu
     type, bind(c) :: c_particle
         real(c_float) :: dx, dy, ux, uy, uz
         integer(c_int32_t) :: grid, q, pid
+    end type
+
+    ! pbpic_particle_f64: the double-precision twin (56 bytes)
+    type, bind(c) :: c_particle_f64
+        real(c_double) :: dx, dy, ux, uy, uz
+        integer(c_int32_t) :: grid, q, pid, pad
+    end type
+
+    ! pbpic_loader: the seeded plasma loaders (kind PBPIC_LOAD_DOUBLE_HARRIS is the
+    ! reference's initparticles / initfields, pic2d.f90:357-648); seed is unsigned in C
+    type, bind(c) :: pbpic_loader
+        integer(c_int32_t) :: kind, ppc
+        real(c_double) :: vthe, vthi, vdrift_e, vdrift_i, lambda, nb, psi0, bguide, b0z, anisotropy
+        integer(c_int64_t) :: seed
+        integer(c_int32_t) :: immobile_ions, reserved
+        real(c_double) :: vthe_bg, vthi_bg
     end type
 
     interface
@@ -163,6 +184,87 @@ module pbpic_gpu
             real(c_double), value :: de_electron, de_ion
             integer(c_int32_t), value :: nbins
             integer(c_int64_t), intent(out) :: counts(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_set_stream(h, stream) bind(c, name="pbpic_set_stream") result(ierr)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, stream
+            integer(c_int) :: ierr
+        end function
+        function pbpic_synchronize(h) bind(c, name="pbpic_synchronize") result(ierr)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int) :: ierr
+        end function
+        function pbpic_init_plasma(h, ld) bind(c, name="pbpic_init_plasma") result(ierr)
+            import :: c_int, c_ptr, pbpic_loader
+            type(c_ptr), value :: h
+            type(pbpic_loader), intent(in) :: ld
+            integer(c_int) :: ierr
+        end function
+        function pbpic_loader_count(h, ld, n) bind(c, name="pbpic_loader_count") result(ierr)
+            import :: c_int, c_ptr, c_int64_t, pbpic_loader
+            type(c_ptr), value :: h
+            type(pbpic_loader), intent(in) :: ld
+            integer(c_int64_t), intent(out) :: n
+            integer(c_int) :: ierr
+        end function
+        function pbpic_num_particles(h, n) bind(c, name="pbpic_num_particles") result(ierr)
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int64_t), intent(out) :: n
+            integer(c_int) :: ierr
+        end function
+        function pbpic_load_particles_f64(h, p, n) bind(c, name="pbpic_load_particles_f64") result(ierr)
+            import :: c_int, c_ptr, c_int64_t, c_particle_f64
+            type(c_ptr), value :: h
+            type(c_particle_f64), intent(in) :: p(*)
+            integer(c_int64_t), value :: n
+            integer(c_int) :: ierr
+        end function
+        function pbpic_store_particles_f64(h, p, cap, n) bind(c, name="pbpic_store_particles_f64") result(ierr)
+            import :: c_int, c_ptr, c_int64_t, c_particle_f64
+            type(c_ptr), value :: h
+            type(c_particle_f64), intent(out) :: p(*)
+            integer(c_int64_t), value :: cap
+            integer(c_int64_t), intent(out) :: n
+            integer(c_int) :: ierr
+        end function
+        ! emfgrid (pic2d.f90:72): (mx+1) x (my+1) nodes of 8 values; the record varies
+        ! fastest, then y, then x
+        function pbpic_store_emfgrid_f64(h, grid8) bind(c, name="pbpic_store_emfgrid_f64") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: grid8(*)
+            integer(c_int) :: ierr
+        end function
+        ! denjr (pic2d.f90:73): jx, jy, jz, rho as 4 planes of mx x (my+1)
+        function pbpic_store_denjr_f64(h, j4) bind(c, name="pbpic_store_denjr_f64") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: j4(*)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_reconnected_flux(h, flux) bind(c, name="pbpic_reconnected_flux") result(ierr)
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: flux
+            integer(c_int) :: ierr
+        end function
+        ! energies and Gauss residual of the rows [y_lo, y_hi) of one y slab
+        function pbpic_energies_rows(h, y_lo, y_hi, wall_lo, wall_hi, e) &
+                bind(c, name="pbpic_energies_rows") result(ierr)
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: y_lo, y_hi, wall_lo, wall_hi
+            real(c_double), intent(out) :: e(4)
+            integer(c_int) :: ierr
+        end function
+        function pbpic_gauss_residual_rows(h, y_lo, y_hi, r) bind(c, name="pbpic_gauss_residual_rows") result(ierr)
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: y_lo, y_hi
+            real(c_double), intent(out) :: r
             integer(c_int) :: ierr
         end function
         function pbpic_last_error() bind(c, name="pbpic_last_error") result(msg)
