@@ -267,6 +267,23 @@ module pbpic_gpu
             real(c_double), intent(out) :: r
             integer(c_int) :: ierr
         end function
+        function pbpic_get_config(h, cfg) bind(c, name="pbpic_get_config") result(ierr)
+            import :: c_int, c_ptr, pbpic_config
+            type(c_ptr), value :: h
+            type(pbpic_config), intent(out) :: cfg
+            integer(c_int) :: ierr
+        end function
+        ! dispersioninfo (pic2d.f90:2124-2142): node values along node rows rows(1:nrows)
+        ! and node columns cols(1:ncols), 0-based indices; out holds nrows*mx*6 then
+        ! ncols*my*6 values, the 6 components varying fastest
+        function pbpic_field_cuts(h, rows, nrows, cols, ncols, out) bind(c, name="pbpic_field_cuts") result(ierr)
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), intent(in) :: rows(*), cols(*)
+            integer(c_int32_t), value :: nrows, ncols
+            real(c_double), intent(out) :: out(*)
+            integer(c_int) :: ierr
+        end function
         function pbpic_last_error() bind(c, name="pbpic_last_error") result(msg)
             import :: c_ptr
             type(c_ptr) :: msg
