@@ -101,3 +101,44 @@ def test_fortran_module_binds_exported_symbols():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) <= set(declared_functions()) | {"pbpic_last_error"}
+
+
+FORTRAN = os.path.join(ROOT, "pbpic_b200", "fortran", "pbpic_gpu.f90")
+_FKIND = {"c_int32_t": ("i", 4), "c_int64_t": ("i", 8), "c_double": ("f", 8), "c_float": ("f", 4)}
+
+
+def fortran_records(text):
+    """name -> [(field, (kind letter, bytes))] of every `type, bind(c)` block."""
+    out = {}
+    for name, body in re.findall(r"type, bind\(c\) :: (\w+)\n(.*?)end type", text, flags=re.S):
+        fields = []
+        for line in body.splitlines():
+            line = line.split("!")[0].strip()
+            if "::" not in line:
+                continue
+            decl, names = line.split("::")
+            kind = _FKIND[re.search(r"\((c_\w+)\)", decl).group(1)]
+            fields += [(n.strip(), kind) for n in names.split(",")]
+        out[name] = fields
+    return out
+
+
+def _ctypes_kind(t):
+    return ("f" if t in (ctypes.c_double, ctypes.c_float) else "i", ctypes.sizeof(t))
+
+
+def test_fortran_module_matches_the_header():
+    """The Fortran module (not compiled here: no Fortran compiler) binds only
+    functions the header declares, and its records list the C structs' fields
+    in order with the same kinds and sizes."""
+    from pbpic_b200 import _lib
+    text = open(FORTRAN).read()
+    names = re.findall(r'bind\(c,\s*name="(pbpic_\w+)"\)', text)
+    assert names and set(names) <= set(declared_functions())
+    recs = fortran_records(text)
+    rename = {"lambda": "lambda_"}
+    for fname, cls in (("pbpic_config", _lib.Config), ("pbpic_loader", _lib.Loader)):
+        got = [(rename.get(n, n), k) for n, k in recs[fname]]
+        assert got == [(n, _ctypes_kind(t)) for n, t in cls._fields_], fname
+    for fname, dt in (("c_particle", _lib.PARTICLE_F32), ("c_particle_f64", _lib.PARTICLE_F64)):
+        assert [(n, k) for n, k in recs[fname]] == [(n, (dt[n].kind, dt[n].itemsize)) for n in dt.names], fname
