@@ -5,10 +5,13 @@
 //
 // Work decomposition: a tile is a run of `tile_rows` cells of one column
 // (contiguous in the cell-sorted order); one block pushes the particles of one
-// tile. Each thread takes 8 consecutive particles per pass, read and written
-// in groups of 4 with 128-bit accesses. Consecutive particles of a sorted
-// array share their cell, so a thread sums the deposit stencils of its
-// particles in registers before touching memory.
+// tile. Each thread takes 8 consecutive particles per pass (4 in the plain
+// form), written in groups of 4 with 128-bit stores; they are read the same way
+// in place, or one by one through the sort's permutation. The mixed form
+// gathers a cell's 4 nodes from the cell's record (k_cell_records), the plain
+// form from the node grid. Consecutive particles of a sorted array share their
+// cell, so a thread sums the deposit stencils of its particles in registers
+// before touching memory.
 //
 // Deposit: the zig-zag move of a particle splits at the relay point into a
 // segment in the old cell and one in the new cell. Everything attached to the
