@@ -78,6 +78,13 @@ typedef struct pbpic_config {
  * sort every 50 steps). pbpic_sort on sorted particles does nothing. This
  * option leaves the sort to the caller, as the reference's pusher does. */
 #define PBPIC_OPT_NO_AUTOSORT 1
+/* Plain form only: evaluate the push's square roots and quotients correctly
+ * rounded in the reference's order (pic2d.f90:969-1028), so that the particle
+ * state after a step is bit-identical to an FP64 evaluation of the reference's
+ * expressions. Without it 1/gamma comes from a reciprocal square root and the
+ * state agrees with that evaluation to a few ulp (1e-15 relative), faster.
+ * Any compat switch implies it. */
+#define PBPIC_OPT_EXACT_FP64 2
 
 /* The reference's `type particle` (pic2d.f90:47-50): 32 bytes. grid is the
  * 1-based cell my*(ix-1)+iy (y fastest), dx, dy the offset from the cell
@@ -255,7 +262,9 @@ int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
  * (about 17 MB, held on every GPU that loads the library until the process
  * exits); larger n is rejected with PBPIC_ECAPACITY. The first call on a device
  * looks up the array's address and should come before any stream capture.
- * Calls share the array: calls that overlap on the GPU race. */
+ * Each call reads the key-range check back to the host, so it returns only
+ * after its stream has finished the sort. Calls share the array: calls that
+ * overlap on the GPU race. */
 #define PBPIC_STATIC_SORT_MAX_KEYS 1048576
 int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t ncells,
                                     int32_t* perm_dev, int32_t* counts_dev, void* stream);
@@ -361,6 +370,12 @@ int pbpic_batch_energies(pbpic_batch* b, double* out);
  * particles, which makes the loss differentiable in nb. No counterpart in the
  * reference (which has no gradients). */
 #define PBPIC_LOSS_MAGNETIC 0 /* sum over steps of dt * magnetic field energy */
+/* sum over steps of the work the electric field does on the particles,
+ * dt * mime / (cva^2 in0) * sum over the Yee grid of J^{n+1/2} . E^n (the
+ * current a step deposits against the E it starts from; the rate at which the
+ * current drains the field energy in the E update, pic2d.f90:742-744). The
+ * reference's own j.E analysis (python/analysis_jdote.py) is a stub. */
+#define PBPIC_LOSS_JDOTE 1
 
 typedef struct pbpic_diff_config {
   int32_t mx, my;       /* cells; conducting walls in y, periodic in x */

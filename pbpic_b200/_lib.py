@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libpbpic.so")
 
 PBPIC_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ECAPACITY", -5: "ESTATE"}
+ERR_INVAL, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_STATE = -1, -2, -3, -4, -5
 
 BC_PERIODIC, BC_CONDUCTING = 0, 1
 FP64_PLAIN, FP32_MIXED = 0, 1
@@ -21,6 +22,7 @@ STATUS_CELL_JUMP, STATUS_NAN, STATUS_UNSORTED = 1, 2, 4
 LOAD_UNIFORM, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_WEIBEL, LOAD_DOUBLE_HARRIS = 0, 1, 2, 3, 4
 FILTER_MARDER, FILTER_CERENKOV = 1, 2
 OPT_NO_AUTOSORT = 1
+OPT_EXACT_FP64 = 2
 
 
 class Config(ctypes.Structure):
@@ -60,7 +62,7 @@ class DiffParams(ctypes.Structure):
     _fields_ = [("psi0", ctypes.c_double), ("nb", ctypes.c_double), ("ti_te", ctypes.c_double)]
 
 
-LOSS_MAGNETIC = 0
+LOSS_MAGNETIC, LOSS_JDOTE = 0, 1
 
 # The reference's `type particle` (pic2d.f90:47-50) and its double-precision twin.
 PARTICLE_F32 = np.dtype([("dx", "<f4"), ("dy", "<f4"), ("ux", "<f4"), ("uy", "<f4"), ("uz", "<f4"),

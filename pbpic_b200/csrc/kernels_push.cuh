@@ -130,10 +130,15 @@ __device__ __forceinline__ void st4(uint32_t* p, const uint32_t (&v)[4]) {
   *reinterpret_cast<uint4*>(p) = make_uint4(v[0], v[1], v[2], v[3]);
 }
 
-// Reciprocal square root and quotient of the push. Plain form: correctly
-// rounded, as the reference's expressions. Mixed form: the hardware
-// reciprocal square root and fast division (deterministic, about 2 ulp).
+// Reciprocal square root and quotient of the push. Plain form, exact order
+// (COMPAT instances): correctly rounded square roots and quotients, as the
+// reference's expressions. Plain form otherwise: 1/gamma from CUDA's double
+// rsqrt, so that the push's chain holds one FP64 division instead of four
+// quotients and two square roots (results within a few ulp of the exact
+// order). Mixed form: the hardware reciprocal square root and fast division
+// (deterministic, about 2 ulp).
 __device__ __forceinline__ float push_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double push_rsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float push_fdiv(float a, float b) { return __fdividef(a, b); }
 
 // Outcome of pushing one particle.
@@ -156,7 +161,9 @@ struct Pushed {
 // Push of one particle whose gather nodes are n00 (ix,iy), n01 (ix,iy+1),
 // n10 (ix+1,iy), n11 (ix+1,iy+1). MIXED is only instantiated with T = float.
 // COMPAT = false compiles the step for a configuration without the compat
-// switches of the push (the rho weights are then the gather weights).
+// switches of the push (the rho weights are then the gather weights) and, in
+// the plain form, forms 1/gamma with rsqrt; COMPAT = true keeps the
+// reference's correctly rounded quotients and square roots, bit for bit.
 template <class T, bool MIXED, bool COMPAT = true>
 __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux,
                                          T puy, T puz, const Node6<T>& n00, const Node6<T>& n01,
@@ -179,7 +186,7 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
   const T umx = A::mad(c1, ex, pux), umy = A::mad(c1, ey, puy), umz = A::mad(c1, ez, puz);
   const T g2m = A::mad(umz, umz, A::mad(umy, umy, A::mad(umx, umx, one)));
   T c2, t2;
-  if constexpr (MIXED) {
+  if constexpr (MIXED || !COMPAT) {
     c2 = A::mul(c0, push_rsqrt(g2m));
   } else {
     c2 = A::div(c0, A::sqrt(g2m));
@@ -208,6 +215,11 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
     gama = A::mul(g2, rg);
     c3 = A::mul(a.dtcva, rg);
     vz = A::mul(uz, rg);  // uz/gamma; cva enters when the fixed-point sum is converted
+  } else if constexpr (!COMPAT) {
+    const T rg = push_rsqrt(g2);
+    gama = A::mul(g2, rg);
+    c3 = A::mul(a.dtcva, rg);              // pic2d.f90:1004
+    vz = A::mul(A::mul(uz, a.cva), rg);    // pic2d.f90:1028
   } else {
     gama = A::sqrt(g2);
     c3 = A::div(a.dtcva, gama);            // pic2d.f90:1004

@@ -20,6 +20,7 @@
 #include "kernels_field.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_push.cuh"
+#include "kernels_push_cells.cuh"
 #include "kernels_slab.cuh"
 #include "kernels_sort.cuh"
 #include "npy_io.h"
@@ -221,6 +222,13 @@ int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
 size_t push_smem_bytes(int ty, bool mixed) {
   if (!mixed) return push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * sizeof(double);
   return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4;
+}
+
+// Dynamic shared memory of k_push_cells: the window (16 planes of ty+3 8-byte
+// sums), the new-cell histogram and, in the mixed form, the crossers' split
+// 32-bit windows.
+size_t push_cells_smem_bytes(int ty, bool mixed) {
+  return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (mixed ? (size_t)16 * (ty + 3) * 4 : 0);
 }
 
 // Lets the plain form's k_push instantiations take more than 48 KB of shared
@@ -502,7 +510,11 @@ int do_push(pbpic_handle* h) {
   if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
   if (MIXED && !p.cg) return fail(PBPIC_ESTATE, "k_push: no per-cell gather records");
   const int nt = PushThreads<T>::value;
-  const bool compat = h->cfg.compat != 0;
+  // sorted input: one warp per cell (kernels_push_cells.cuh); smem: window, histogram, crossers' windows
+  const int ct = PBPIC_CPUSH_THREADS;
+  const size_t csmem = push_cells_smem_bytes(h->TY, MIXED);
+  // the compat instances also carry the plain form's exact-order arithmetic
+  const bool compat = h->cfg.compat != 0 || (!MIXED && (h->cfg.options & PBPIC_OPT_EXACT_FP64));
   if (h->lazy) {  // read through the sort's permutation, write in cell order to the other buffer
     if (!hist) return fail(PBPIC_ESTATE, "k_push: a permuted input needs the sort's tables");
     const int o = 1 - h->cur;
@@ -515,13 +527,17 @@ int do_push(pbpic_handle* h) {
     p.uz_o = P<T>(h, o, 4);
     p.pid_i = h->pid[h->cur];
     p.pid_o = h->pid[o];
-    if (!compat) k_push<T, MIXED, true, false, true><<<h->ntiles, nt, smem, s>>>(p);
+    if (PBPIC_PUSH_CELLS && !compat) k_push_cells<T, MIXED, false, true><<<h->ntiles, ct, csmem, s>>>(p);
+    else if (PBPIC_PUSH_CELLS) k_push_cells<T, MIXED, true, true><<<h->ntiles, ct, csmem, s>>>(p);
+    else if (!compat) k_push<T, MIXED, true, false, true><<<h->ntiles, nt, smem, s>>>(p);
     else k_push<T, MIXED, true, true, true><<<h->ntiles, nt, smem, s>>>(p);
     CKLAUNCH("k_push");
     h->cur = o;
     h->lazy = false;
   } else {
-    if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
+    if (PBPIC_PUSH_CELLS && hist && !compat) k_push_cells<T, MIXED, false, false><<<h->ntiles, ct, csmem, s>>>(p);
+    else if (PBPIC_PUSH_CELLS && hist) k_push_cells<T, MIXED, true, false><<<h->ntiles, ct, csmem, s>>>(p);
+    else if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
     else if (hist) k_push<T, MIXED, true, true><<<h->ntiles, nt, smem, s>>>(p);
     else if (!compat) k_push<T, MIXED, false, false><<<h->ntiles, nt, smem, s>>>(p);
     else k_push<T, MIXED, false, true><<<h->ntiles, nt, smem, s>>>(p);
@@ -903,7 +919,7 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
     return fail(PBPIC_EINVAL, "unknown precision");
   if (c.capacity < 0 || c.capacity > 0x7fffff00ll) return fail(PBPIC_EINVAL, "capacity must be in [0, 2^31)");
   if (c.compat & ~7) return fail(PBPIC_EINVAL, "unknown compat bits");
-  if (c.options & ~PBPIC_OPT_NO_AUTOSORT) return fail(PBPIC_EINVAL, "unknown option bits");
+  if (c.options & ~(PBPIC_OPT_NO_AUTOSORT | PBPIC_OPT_EXACT_FP64)) return fail(PBPIC_EINVAL, "unknown option bits");
   const double cfl = c.cva * c.dt * sqrt(1.0 / (c.dx * c.dx) + 1.0 / (c.dy * c.dy));
   if (!(cfl < 1.0)) return fail(PBPIC_EINVAL, "time step violates the CFL condition c*dt*sqrt(1/dx^2+1/dy^2) < 1");
   if (c.cva * c.dt / std::min(c.dx, c.dy) >= 1.0)
@@ -1351,7 +1367,9 @@ int pbpic_counting_sort_keys(const int32_t* keys_dev, int64_t n, int32_t ncells,
 // array until the process exits. Host code cannot use the array's name as a
 // device address, so the first call on each device (with that device current)
 // looks the address up with cudaGetSymbolAddress and keeps it; make that first
-// call before any stream capture. All calls share the array and it keeps the
+// call before any stream capture. Each call copies the key-range status back
+// to the host and waits for its stream, so it returns with the sort finished.
+// All calls share the array and it keeps the
 // last call's contents: the only word that must start at zero (the key-range
 // status) is cleared on every call, and calls that overlap on the GPU (on
 // different streams or host threads) race on the array.
@@ -2218,6 +2236,7 @@ int band_extract_sorted(pbpic_handle* h, int y_lo, int y_hi, int my_global, int 
   CK(cudaStreamSynchronize(s));
   if (nout) *nout = total;
   if (total > cap) return fail(PBPIC_ECAPACITY, "the band holds more particles than the destination");
+  if (total > 0 && !dst) return fail(PBPIC_EINVAL, "null band destination");
   const int b = h->cur;
   if (total > 0) {
     k_band_out_sorted<T, T><<<grid_for(total, 256), 256, 0, s>>>(
@@ -2239,6 +2258,7 @@ int do_band_extract(pbpic_handle* h, int y_lo, int y_hi, int my_global, int row_
   TRY(band_positions(h, y_lo, y_hi, &c));
   if (nout) *nout = c;
   if (c > cap) return fail(PBPIC_ECAPACITY, "the band holds more particles than the destination");
+  if (c > 0 && !dst) return fail(PBPIC_EINVAL, "null band destination");
   const int b = h->cur;
   if (h->n > 0 && c > 0) {
     k_band_out<T, T><<<grid_for(h->n, 256), 256, 0, h->stream>>>(h->n, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),

@@ -86,15 +86,32 @@ class GpuEngine:
         self.rec = L.PARTICLE_F32 if precision in ("fp32", "mixed") else L.PARTICLE_F64
         self.ftype = torch.float32 if precision in ("fp32", "mixed") else torch.float64
         self.lib = L.lib()
+        self.bands = {}  # outgoing band buffers, one per direction, grown as needed
 
     # particles
-    def extract(self, y_lo, y_hi):
+    def extract(self, y_lo, y_hi, slot=0):
+        """The particles of rows [y_lo, y_hi) as reference records in a device
+        buffer kept for `slot` (one per direction), valid until the next
+        extract into the same slot. A band holds a few rows' particles, so the
+        buffer is sized from the band's own count (the library reports it when
+        the buffer is too small) with a quarter to spare, not from the slab."""
         n = ctypes.c_int64()
-        cap = max(self.sim.num_particles(), 1)
-        buf = self.torch.empty(cap * self.rec.itemsize, dtype=self.torch.uint8, device="cuda")
-        L.check(self.lib.pbpic_band_extract(self.sim.handle, y_lo, y_hi, self.lay.my, self.lay.row_offset,
-                                            ctypes.c_void_p(buf.data_ptr()), cap, ctypes.byref(n)))
-        return buf[: n.value * self.rec.itemsize]
+        size = self.rec.itemsize
+        buf = self.bands.get(slot)
+        cap = 0 if buf is None else buf.numel() // size
+        dst = ctypes.c_void_p(buf.data_ptr()) if cap else None
+        rc = self.lib.pbpic_band_extract(self.sim.handle, y_lo, y_hi, self.lay.my, self.lay.row_offset, dst, cap,
+                                         ctypes.byref(n))
+        if rc == L.ERR_CAPACITY:
+            cap = n.value + n.value // 4 + 256
+            buf = self.torch.empty(cap * size, dtype=self.torch.uint8, device="cuda")
+            self.bands[slot] = buf
+            rc = self.lib.pbpic_band_extract(self.sim.handle, y_lo, y_hi, self.lay.my, self.lay.row_offset,
+                                             ctypes.c_void_p(buf.data_ptr()), cap, ctypes.byref(n))
+        L.check(rc)
+        if n.value == 0:
+            return self.empty_band()
+        return buf[: n.value * size]
 
     def keep(self, y_lo, y_hi):
         L.check(self.lib.pbpic_band_keep(self.sim.handle, y_lo, y_hi))
@@ -148,6 +165,11 @@ class GpuEngine:
         v = ctypes.c_double()
         L.check(self.lib.pbpic_gauss_residual_rows(self.sim.handle, self.lay.lo, self.lay.hi, ctypes.byref(v)))
         return v.value
+
+    def own_count(self):
+        """Particles in the slab's own rows (ghosts excluded)."""
+        c = self.sim.cell_counts().reshape(self.sim.mx, self.lay.my_local)
+        return int(c[:, self.lay.lo:self.lay.hi].sum())
 
 
 class InProcess:
@@ -243,8 +265,8 @@ class SlabRun:
         out = {}
         for r, e in self.slabs.items():
             lay = e.lay
-            to_down = e.extract(lay.lo, lay.lo + lay.g) if lay.has_down else None
-            to_up = e.extract(lay.hi - lay.g, lay.hi) if lay.has_up else None
+            to_down = e.extract(lay.lo, lay.lo + lay.g, 0) if lay.has_down else None
+            to_up = e.extract(lay.hi - lay.g, lay.hi, 1) if lay.has_up else None
             out[r] = (to_down, to_up)
         inc = self.t.exchange(self.slabs, out)
         for r, e in self.slabs.items():

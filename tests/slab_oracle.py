@@ -23,7 +23,7 @@ class OracleEngine:
         g = p["grid"].astype(np.int64) - 1
         return g // self.lay.my_local, g % self.lay.my_local
 
-    def extract(self, y_lo, y_hi):
+    def extract(self, y_lo, y_hi, slot=0):
         p = self.o.particles()
         ix, iy = self._rows(p)
         m = (iy >= y_lo) & (iy < y_hi)
@@ -72,6 +72,36 @@ class OracleEngine:
 
     def sort(self):
         self.o.countingsort()
+
+    def gauss_residual(self):
+        """max |div E / cva^2 - in0 rho| over the slab's own node rows (walls:
+        interior rows), rho the bilinear charge of the particles -- the
+        definition of pbpic_gauss_residual_rows."""
+        c = self.cfg
+        mx, my = self.mx, self.lay.my_local
+        p = self.o.particles()
+        g = p["grid"].astype(np.int64) - 1
+        ix, iy = g // my, g % my
+        ax, ay = 0.5 + p["dx"], 0.5 + p["dy"]
+        q = p["q"].astype(np.float64)
+        rho = np.zeros((mx, my + 1))
+        ip = (ix + 1) % mx
+        jp = iy + 1
+        if c["ybc"] == 0:
+            jp = np.where(jp == my, 0, jp)
+        for xi, yj, w in ((ix, iy, (1 - ax) * (1 - ay)), (ip, iy, ax * (1 - ay)), (ix, jp, (1 - ax) * ay),
+                          (ip, jp, ax * ay)):
+            np.add.at(rho, (xi, yj), q * w)
+        f = self.o.fields()
+        ex, ey = f[0], f[1]
+        j0 = max(self.lay.lo, 0 if c["ybc"] == 0 else 1)
+        j1 = min(self.lay.hi, my)
+        j = np.arange(j0, j1)
+        dive = (ex[:, j] - np.roll(ex, 1, axis=0)[:, j]) / c["dx"] + (ey[:, j] - ey[:, (j - 1) % my]) / c["dy"]
+        return float(np.abs(dive / c["cva"] ** 2 - c["in0"] * rho[:, j]).max()) if len(j) else 0.0
+
+    def own_count(self):
+        return len(self.own_particles())
 
     def own_particles(self):
         p = self.o.particles()
