@@ -1,9 +1,11 @@
 """PyTorch autograd wrapper of the differentiable form (pbpic_diff_* in the C ABI).
 
-HarrisLoss.apply(params, engine) returns the time-integrated magnetic energy of
-a GEM Harris sheet run as a function of params = (psi0, nb, Ti/Te), a float64
-tensor of 3 values; its backward pass runs the library's discrete adjoint
-(checkpointed, recomputed between checkpoints) and returns d loss / d params.
+HarrisLoss.apply(params, engine) returns the engine's loss of a GEM Harris sheet
+run -- the time-integrated magnetic energy, or the time-integrated work j.E the
+electric field does on the particles -- as a function of params = (psi0, nb,
+Ti/Te), a float64 tensor of 3 values; its backward pass runs the library's
+discrete adjoint (checkpointed, recomputed between checkpoints) and returns
+d loss / d params.
 """
 import ctypes
 
@@ -16,12 +18,13 @@ class DiffEngine:
     """One checkpointed forward/adjoint engine on the current CUDA device."""
 
     def __init__(self, mx, my, ppc, nsteps, checkpoint_every, precision="fp32", dx=0.1, mime=25.0, wpe_wce=2.0,
-                 lam=0.5, nb0=0.2, cfl=0.5, seed=3):
+                 lam=0.5, nb0=0.2, cfl=0.5, seed=3, loss="magnetic"):
         self._lib = L.lib()
         prec = {"fp64": L.FP64_PLAIN, "fp32": L.FP32_MIXED}[precision]
+        kind = {"magnetic": L.LOSS_MAGNETIC, "jdote": L.LOSS_JDOTE}[loss]
         self.cfg = L.DiffConfig(mx=mx, my=my, ppc=ppc, precision=prec, dx=dx, mime=mime, wpe_wce=wpe_wce,
                                 lambda_=lam, nb0=nb0, cfl=cfl, nsteps=nsteps, checkpoint_every=checkpoint_every,
-                                loss=L.LOSS_MAGNETIC, seed=seed)
+                                loss=kind, seed=seed)
         self._h = ctypes.c_void_p()
         L.check(self._lib.pbpic_diff_create(ctypes.byref(self.cfg), ctypes.byref(self._h)))
 

@@ -420,6 +420,47 @@ __global__ void k_loss_b(int mx, int my, int ybc, const T* ng, double scale, dou
   if (threadIdx.x == 0 && loss) atomicAdd(loss, scale * s);
 }
 
+// The j.E loss of one step and its adjoint seeds: sum over the Yee entries
+// (ex: node rows, off the walls; ey, ez: half rows) of J_k E_k, J the step's
+// normalised current (jacc * jscale), E the fields the step starts from.
+// With jbar/fbar_e, also adds scale * E to the current adjoint and scale * J to
+// the E adjoint (3 planes each, mx x S).
+template <class T, class Acc>
+__global__ void k_loss_jdote(int mx, int my, int S, int ybc, const void* jacc, double jscale, const T* ex,
+                             const T* ey, const T* ez, double scale, double* loss, double* jbar, double* fbar_e) {
+  __shared__ double red[32];
+  const Acc* J = reinterpret_cast<const Acc*>(jacc);
+  const long long plane = (long long)mx * S;
+  const int rows = ybc == 0 ? my : my + 1;
+  const long long n = (long long)mx * rows;
+  double s = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / rows), j = (int)(k - (long long)i * rows);
+    const long long o = (long long)i * S + j;
+    if (!(ybc == 1 && (j == 0 || j == my))) {
+      const double jx = (double)J[o] * jscale, e = (double)ex[o];
+      s += jx * e;
+      if (jbar) {
+        jbar[o] += scale * e;
+        fbar_e[o] += scale * jx;
+      }
+    }
+    if (j < my) {
+      const double jy = (double)J[plane + o] * jscale, ey_ = (double)ey[o];
+      const double jz = (double)J[2 * plane + o] * jscale, ez_ = (double)ez[o];
+      s += jy * ey_ + jz * ez_;
+      if (jbar) {
+        jbar[plane + o] += scale * ey_;
+        jbar[2 * plane + o] += scale * ez_;
+        fbar_e[plane + o] += scale * jy;
+        fbar_e[2 * plane + o] += scale * jz;
+      }
+    }
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0 && loss) atomicAdd(loss, scale * s);
+}
+
 // d loss / d (Ti/Te) through the loaded momenta. The loader sets
 // u = g uth(tau) + U(tau) (U: the sheet drift along z), so with g recovered
 // from the loaded u, du/dtau = g duth/dtau + dU/dtau, contracted here with the

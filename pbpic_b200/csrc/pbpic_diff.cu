@@ -73,6 +73,7 @@ struct pbpic_diff {
   double* jbar = nullptr;  // 3 planes
   double* gbar = nullptr;  // node adjoint
   double* scal = nullptr;  // [0] loss, [1] d loss / d omega, [2] d loss / d tau
+  void* jseg = nullptr;    // j.E loss: the current of each step of the recomputed segment (3 planes each)
   pbpic_diff_params last{};
   bool have_forward = false;
   std::vector<void*> allocs;
@@ -194,6 +195,28 @@ FieldParams<T> field_params(const pbpic_diff* d, const Slot& s) {
 
 double loss_scale(const pbpic_diff* d) { return d->dt * 0.5 * d->cfg.mime / (d->cva * d->cva * d->in0); }
 
+// j.E loss: dt * mime / (cva^2 in0) * sum J . E, the work done on the particles
+// in the units of the field energy (the E update drains cva^2 J per unit time
+// from fields whose energy is mime / (2 cva^4 in0) sum E^2).
+double jdote_scale(const pbpic_diff* d) { return d->dt * d->cfg.mime / (d->cva * d->cva * d->in0); }
+double jdote_jscale(const pbpic_diff* d) { return d->f32 ? d->in0 * FIX_INV : d->in0; }
+
+// The j.E loss of the step whose current is in `jacc` and whose starting
+// fields are the slot's; with jbar/fbar_e, its adjoint seeds.
+template <class T>
+int loss_jdote(pbpic_diff* d, const Slot& s, const void* jacc, double* loss, double* jbar, double* fbar_e) {
+  View<T> v = view<T>(d, s);
+  const int g = grid_of((int64_t)d->mx * (d->my + 1));
+  if (d->f32)
+    k_loss_jdote<T, long long><<<g, 256>>>(d->mx, d->my, d->S, PBPIC_BC_CONDUCTING, jacc, jdote_jscale(d), v.f[0],
+                                           v.f[1], v.f[2], jdote_scale(d), loss, jbar, fbar_e);
+  else
+    k_loss_jdote<T, double><<<g, 256>>>(d->mx, d->my, d->S, PBPIC_BC_CONDUCTING, jacc, jdote_jscale(d), v.f[0],
+                                        v.f[1], v.f[2], jdote_scale(d), loss, jbar, fbar_e);
+  DLAUNCH("k_loss_jdote");
+  return PBPIC_OK;
+}
+
 // Node grid of a slot's fields into d->ng.
 template <class T>
 int nodes(pbpic_diff* d, const Slot& s) {
@@ -203,9 +226,10 @@ int nodes(pbpic_diff* d, const Slot& s) {
   return PBPIC_OK;
 }
 
-// One forward step of a slot in place; adds the step's loss to scal[0].
+// One forward step of a slot in place; adds the step's loss to scal[0]. With
+// the j.E loss and `jkeep`, also keeps the step's current (3 planes) there.
 template <class T>
-int step(pbpic_diff* d, const Slot& s, double omega) {
+int step(pbpic_diff* d, const Slot& s, double omega, void* jkeep = nullptr) {
   DTRY(nodes<T>(d, s));
   DCK(cudaMemsetAsync(d->jacc, 0, (size_t)4 * plane(d) * 8));
   DiffParams<T> dp;
@@ -217,6 +241,11 @@ int step(pbpic_diff* d, const Slot& s, double omega) {
   dp.in0 = d->in0;
   k_dpush<T><<<grid_of(d->n, 148 * 16), 256>>>(dp);
   DLAUNCH("k_dpush");
+  const bool jdote = d->cfg.loss == PBPIC_LOSS_JDOTE;
+  if (jdote) {
+    DTRY(loss_jdote<T>(d, s, d->jacc, d->scal, nullptr, nullptr));
+    if (jkeep) DCK(cudaMemcpyAsync(jkeep, d->jacc, (size_t)3 * plane(d) * 8, cudaMemcpyDeviceToDevice));
+  }
   FieldParams<T> a = field_params<T>(d, s);
   const int g = grid_of((int64_t)d->mx * (d->my + 1));
   k_bhalf<T><<<g, 256>>>(a);
@@ -227,9 +256,11 @@ int step(pbpic_diff* d, const Slot& s, double omega) {
   k_bhalf<T><<<g, 256>>>(a);
   DLAUNCH("k_bhalf");
   DTRY(nodes<T>(d, s));
-  k_loss_b<T><<<grid_of((int64_t)(d->mx + 1) * (d->my + 1)), 256>>>(d->mx, d->my, 1, (const T*)d->ng,
-                                                                     loss_scale(d), d->scal, nullptr);
-  DLAUNCH("k_loss_b");
+  if (!jdote) {
+    k_loss_b<T><<<grid_of((int64_t)(d->mx + 1) * (d->my + 1)), 256>>>(d->mx, d->my, 1, (const T*)d->ng,
+                                                                       loss_scale(d), d->scal, nullptr);
+    DLAUNCH("k_loss_b");
+  }
   return PBPIC_OK;
 }
 
@@ -331,6 +362,8 @@ int backward(pbpic_diff* d, double grad[3]) {
   const double omega = d->last.nb / d->cfg.nb0;
   const int64_t pl = plane(d);
   const size_t nodes_bytes = (size_t)(d->mx + 1) * (d->my + 1) * 8 * sizeof(double);
+  const bool jdote = d->cfg.loss == PBPIC_LOSS_JDOTE;
+  const size_t jbytes = (size_t)3 * pl * 8;
   for (int k = 0; k < 5; ++k) DCK(cudaMemset(d->lam[0][k], 0, (size_t)d->n * d->tsz));
   DCK(cudaMemset(d->fbar, 0, (size_t)6 * pl * sizeof(double)));
   DCK(cudaMemset(d->scal + 1, 0, 3 * sizeof(double)));
@@ -343,22 +376,26 @@ int backward(pbpic_diff* d, double grad[3]) {
     DTRY(copy_slot(d, d->seg[0], d->ck[sg]));
     for (int m = 0; m < s1 - s0; ++m) {  // recompute the segment, keeping every state
       DTRY(copy_slot(d, d->seg[m + 1], d->seg[m]));
-      DTRY(step<T>(d, d->seg[m + 1], omega));
+      DTRY(step<T>(d, d->seg[m + 1], omega, jdote ? (char*)d->jseg + m * jbytes : nullptr));
     }
     for (int it = s1 - 1; it >= s0; --it) {
       const int m = it - s0;
-      // loss of step it+1: seed the adjoint of the fields after the step
-      DTRY(nodes<T>(d, d->seg[m + 1]));
-      DCK(cudaMemsetAsync(d->gbar, 0, nodes_bytes));
-      k_loss_b<T><<<gn, 256>>>(d->mx, d->my, 1, (const T*)d->ng, loss_scale(d), nullptr, d->gbar);
-      DLAUNCH("k_loss_b");
-      k_adj_nodes<<<gn, 256>>>(af, d->gbar);
-      DLAUNCH("k_adj_nodes");
+      if (!jdote) {  // magnetic loss of step it+1: seed the adjoint of the fields after the step
+        DTRY(nodes<T>(d, d->seg[m + 1]));
+        DCK(cudaMemsetAsync(d->gbar, 0, nodes_bytes));
+        k_loss_b<T><<<gn, 256>>>(d->mx, d->my, 1, (const T*)d->ng, loss_scale(d), nullptr, d->gbar);
+        DLAUNCH("k_loss_b");
+        k_adj_nodes<<<gn, 256>>>(af, d->gbar);
+        DLAUNCH("k_adj_nodes");
+      }
       // transposed field solve: B half step, E full step, B half step in reverse
       k_adj_bhalf<<<gf, 256>>>(af);
       DLAUNCH("k_adj_bhalf");
       k_adj_efull<<<gf, 256>>>(af);
       DLAUNCH("k_adj_efull");
+      // j.E loss of step it: E (the step's start) into the current adjoint, the
+      // step's current into the adjoint of that E
+      if (jdote) DTRY(loss_jdote<T>(d, d->seg[m], (char*)d->jseg + m * jbytes, nullptr, d->jbar, d->fbar));
       k_zero_wall_ex<<<grid_of(d->mx), 256>>>(af);
       DLAUNCH("k_zero_wall_ex");
       k_adj_bhalf<<<gf, 256>>>(af);
@@ -444,7 +481,7 @@ int pbpic_diff_create(const pbpic_diff_config* cfg, pbpic_diff** out) {
   if (c.precision != PBPIC_FP64_PLAIN && c.precision != PBPIC_FP32_MIXED)
     return pbpic_internal_fail(PBPIC_EINVAL, "unknown precision");
   if (c.nsteps <= 0 || c.checkpoint_every <= 0) return pbpic_internal_fail(PBPIC_EINVAL, "nsteps and checkpoint_every must be positive");
-  if (c.loss != PBPIC_LOSS_MAGNETIC) return pbpic_internal_fail(PBPIC_EINVAL, "unknown loss");
+  if (c.loss != PBPIC_LOSS_MAGNETIC && c.loss != PBPIC_LOSS_JDOTE) return pbpic_internal_fail(PBPIC_EINVAL, "unknown loss");
   if (!(c.dx > 0 && c.mime > 0 && c.wpe_wce > 0 && c.lambda > 0 && c.nb0 > 0 && c.cfl > 0 && c.cfl < 1))
     return pbpic_internal_fail(PBPIC_EINVAL, "dx, mime, wpe_wce, lambda, nb0 must be positive and 0 < cfl < 1");
   if ((int64_t)2 * c.ppc * c.mx * c.my > 0x7fffff00ll) return pbpic_internal_fail(PBPIC_EINVAL, "too many particles");
@@ -490,6 +527,7 @@ int pbpic_diff_create(const pbpic_diff_config* cfg, pbpic_diff** out) {
   A((void**)&d->jbar, (size_t)3 * plane(d) * sizeof(double));
   A((void**)&d->gbar, (size_t)(c.mx + 1) * (c.my + 1) * 8 * sizeof(double));
   A((void**)&d->scal, 4 * sizeof(double));
+  if (c.loss == PBPIC_LOSS_JDOTE) A(&d->jseg, (size_t)c.checkpoint_every * 3 * plane(d) * 8);
   if (r != PBPIC_OK) {
     pbpic_diff_destroy(d);
     return r;
