@@ -10,9 +10,13 @@ untimed, max over ranks. The particle state (2.5 GB mixed, 4.6 GB plain) is
 far larger than L2, so no flush is needed between steps.
 
 --impl reference times the CPU restatement of the reference (oracle/, OpenMP
-over all host threads) on a bounded sample of the same workload.
-Multi-GPU: independent replicas per rank (the single-domain step does not
-shard here), weak scaling.
+over all host threads, FP64) on the whole workload with the same warm-up and
+timed steps; the GPU arm's cpu_baseline times it on a bounded sample.
+Multi-GPU (N > 1, one process per GPU): the reference's y-slab decomposition,
+weak-scaled -- the Harris sheet on 1024 x (512 N) cells, 512 own rows per
+rank, ghost bands and ghost field rows exchanged with the neighbours over
+NCCL point-to-point every step (pbpic_b200/slab.py); --replicas runs N
+independent replicas instead. --slabs runs the slab path at one GPU too.
 """
 import argparse
 import json
@@ -37,7 +41,7 @@ PUSH_DRAM_BYTES_PER_PARTICLE = 61.0
 UNIT = "particle-steps/s"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
@@ -50,7 +54,11 @@ def parse():
     ap.add_argument("--sort-every", type=int, default=1)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=20)
-    return ap.parse_args()
+    ap.add_argument("--slabs", action="store_true",
+                    help="run the y-slab decomposition also at one GPU (it is the default for N > 1)")
+    ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of y slabs")
+    ap.add_argument("--slab-rows", type=int, default=512, help="own cell rows per rank of the y-slab run")
+    return ap.parse_args(argv)
 
 
 def workload(name, seed_offset=0):
@@ -58,6 +66,32 @@ def workload(name, seed_offset=0):
     cfg, ld = configs.WORKLOADS[name]()
     ld = dict(ld, seed=ld["seed"] + seed_offset)
     return cfg, ld
+
+
+def workload_kind(name):
+    """What the workload's plasma is, in words."""
+    if name.startswith("double_harris"):
+        return "double Harris sheet (the reference's own run)"
+    if name.startswith("harris"):
+        return "GEM Harris sheet"
+    return "uniform periodic plasma"
+
+
+L2_BYTES = 126e6  # B200 L2
+
+
+def workload_config(name, n):
+    """The `config` object of a workload: its grid, particles, boundaries and
+    whether its particle state exceeds L2 (no flush needed between steps)."""
+    cfg, ld = workload(name)
+    s32, s64 = 24.0 * n, 44.0 * n
+    if s32 > L2_BYTES:
+        l2 = f"inputs larger than L2 (particle state {s32 / 1e9:.2f} GB FP32, {s64 / 1e9:.2f} GB FP64; L2 126 MB)"
+    else:
+        l2 = f"particle state {s32 / 1e6:.0f} MB FP32 fits in L2 (126 MB); no flush between steps"
+    return {"workload": name, "grid": f"{cfg['mx']}x{cfg['my']}", "particles": n,
+            "ppc_per_species": ld["ppc"], "ybc": "conducting" if cfg["ybc"] == 1 else "periodic",
+            "xbc": "periodic", "seed": ld["seed"], "l2": l2}
 
 
 # HBM3e of an HGX B200 as specified (the roofline's denominator is the measured copy bandwidth)
@@ -290,6 +324,219 @@ def run_ensemble(args):
                     gauss=gauss, status=status)
 
 
+# ------------------------------------------------------------- y slabs (N > 1)
+def slab_workload(world, rows=512, mx=1024, ppc=100, seed=1):
+    """The benchmark's Harris sheet weak-scaled over y slabs: mx x (rows * world)
+    cells of 0.1 d_i, 100 particles per cell per species, conducting walls in
+    y, the sheet in the middle of the global domain; each rank owns `rows` rows."""
+    from pbpic_b200 import configs
+    return configs.harris(mx, rows * world, ppc, seed)
+
+
+def gpu_slab_engine(cfg, ld, lay, precision="fp32"):
+    """This rank's slab of the global plasma on its GPU: the loader draws the
+    whole plasma on the device (by pair index, so every rank draws the same
+    one), the slab's own rows and field rows are cut out with the band and
+    row API, the global handle is freed, and the slab handle is filled from
+    the cut. Returns the engine (ghost bands are filled by SlabRun.start)."""
+    import ctypes
+
+    import torch
+
+    from pbpic_b200 import _lib as L
+    from pbpic_b200.sim import Simulation
+    from pbpic_b200.slab import GpuEngine
+    lib = L.lib()
+    rec = L.PARTICLE_F32 if precision == "fp32" else L.PARTICLE_F64
+    ftype = torch.float32 if precision == "fp32" else torch.float64
+    n = Simulation(**cfg, precision=precision, capacity=1).loader_count(**ld)
+    rows = lay.own + (1 if lay.wall_hi >= 0 else 0)  # the top wall's node row on the last slab
+    cnt = ctypes.c_int64()
+    with Simulation(**cfg, precision=precision, capacity=n) as g:
+        g.init_plasma(**ld)
+        rc = lib.pbpic_band_extract(g.handle, lay.y0, lay.y1, lay.my, 0, None, 0, ctypes.byref(cnt))
+        if rc not in (L.PBPIC_OK, L.ERR_CAPACITY):
+            L.check(rc)
+        own = cnt.value
+        band = torch.empty(max(own, 1) * rec.itemsize, dtype=torch.uint8, device="cuda")
+        L.check(lib.pbpic_band_extract(g.handle, lay.y0, lay.y1, lay.my, 0, ctypes.c_void_p(band.data_ptr()), own,
+                                       ctypes.byref(cnt)))
+        f = torch.empty(6 * cfg["mx"] * rows, dtype=ftype, device="cuda")
+        L.check(lib.pbpic_field_rows_get(g.handle, lay.y0, rows, ctypes.c_void_p(f.data_ptr())))
+    # own particles, ghost bands of up to 8 rows (a sheet row holds up to 6x the mean) and slack
+    cap = own + 8 * 6 * (own // max(lay.own, 1)) + (1 << 20)
+    e = GpuEngine(cfg, lay, precision, capacity=cap)
+    e.append(band[: own * rec.itemsize], lay.row_offset)
+    del band
+    e.set_field_rows(lay.lo, rows, f)
+    return e
+
+
+class CudaClock:
+    """Device time of a region on the current stream (CUDA events)."""
+
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+
+    def sync(self):
+        self.torch.cuda.synchronize()
+
+    def start(self):
+        self.a.record()
+
+    def stop(self):
+        self.b.record()
+        self.b.synchronize()
+        return self.a.elapsed_time(self.b)
+
+
+class HostClock:
+    """Wall time of a region (CPU engines)."""
+
+    def sync(self):
+        pass
+
+    def start(self):
+        self.t0 = time.perf_counter()
+
+    def stop(self):
+        return 1e3 * (time.perf_counter() - self.t0)
+
+
+def run_slabs(ranks, transport, engine, steps, warmup, clock, counter=None):
+    """The y-slab step on every rank: `warmup` untimed steps, then `steps`
+    timed ones (push, field solve, ghost-band and ghost-row exchange with the
+    neighbours, sort), a barrier and a synchronisation on both sides, the
+    slowest rank's time. Work units are the own particles of every rank (the
+    ghosts each rank also pushes are redundant work). Every rank returns the
+    same dict."""
+    from pbpic_b200.slab import SlabRun
+    run = SlabRun({ranks.rank: engine}, transport)
+    run.start()
+    run.step(warmup)
+    clock.sync()
+    ranks.barrier()
+    l0 = counter() if counter else 0
+    clock.start()
+    run.step(steps)
+    ms = clock.stop()
+    launches = (counter() - l0) if counter else None
+    ranks.barrier()
+    ms = ranks.max(ms)
+    own = float(transport.allreduce([engine.own_count()], "sum")[0])
+    en = run.energies()
+    gauss = run.gauss_residual()
+    return dict(ms=ms, own=own, value=own * steps / (ms * 1e-3), energies=en.tolist(), gauss=gauss,
+                launches=launches)
+
+
+def run_slabs_e2e(ranks, transport, cfg, lay, host_rec, fields, steps, make_engine):
+    """The y-slab step end to end: each rank's own particle records go from
+    pinned host memory to its GPU (H2D) and into a fresh slab, the ghost bands
+    are exchanged, `steps` steps run with the all-reduced energies read back
+    to the host after every step, and the own particles come back to pinned
+    host memory (D2H). Wall time, the slowest rank's."""
+    import torch
+
+    from pbpic_b200.slab import SlabRun
+    e = make_engine()
+    dev = torch.empty(host_rec.numel(), dtype=torch.uint8, device="cuda")
+    out = torch.empty_like(host_rec).pin_memory()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    t0 = time.perf_counter()
+    dev.copy_(host_rec, non_blocking=True)
+    e.append(dev, lay.row_offset)
+    e.set_field_rows(lay.lo, fields.numel() // (6 * cfg["mx"]), fields)
+    run = SlabRun({ranks.rank: e}, transport)
+    run.start()
+    for _ in range(steps):
+        run.step(1)
+        run.energies()
+    back = e.extract(lay.lo, lay.hi, 2)
+    out[: back.numel()].copy_(back)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    ranks.barrier()
+    return ranks.max(dt), host_rec.numel(), back.numel()
+
+
+def slab_line(args, ranks):
+    """The JSON line of the y-slab run on N GPUs (one slab per rank, NCCL
+    point-to-point exchanges between neighbours, FP32 mixed form)."""
+    import torch
+
+    from pbpic_b200.slab import Layout, TorchDist
+    dev = ranks.local_rank
+    torch.cuda.set_device(dev)
+    cfg, ld = slab_workload(ranks.world, rows=args.slab_rows)
+    lay = Layout(cfg["my"], ranks.world, ranks.rank, cfg["ybc"])
+    transport = TorchDist(ranks.dist, f"cuda:{dev}") if ranks.dist is not None else SelfTransport()
+    import pbpic_b200
+    eng = gpu_slab_engine(cfg, ld, lay)
+    sampler = ClockSampler(dev)
+    sampler.active = True
+    r = run_slabs(ranks, transport, eng, args.steps, args.warmup, CudaClock(), pbpic_b200.kernel_launches)
+    sampler.active = False
+    clocks = sampler.stop()
+    e2e = None
+    if not args.no_e2e:
+        rows = lay.own + (1 if lay.wall_hi >= 0 else 0)
+        band = eng.extract(lay.lo, lay.hi, 2)
+        host = torch.empty(band.numel(), dtype=torch.uint8).pin_memory()
+        host.copy_(band)
+        fields = eng.field_rows(lay.lo, rows).clone()
+        cap = eng.sim.cfg.capacity
+        del band, eng
+        torch.cuda.empty_cache()
+        from pbpic_b200.slab import GpuEngine
+        sec, h2d, d2h = run_slabs_e2e(ranks, transport, cfg, lay, host, fields, args.steps,
+                                      lambda: GpuEngine(cfg, lay, "fp32", capacity=cap))
+        tot = transport.allreduce([h2d, d2h], "sum")
+        e2e = {"value": r["own"] * args.steps / sec, "unit": UNIT, "h2d_bytes_per_step": float(tot[0]) / args.steps,
+               "d2h_bytes_per_step": float(tot[1]) / args.steps + 32.0, "K": args.steps,
+               "what": "every rank: H2D of its own particle records (pinned) into a fresh slab, ghost-band exchange, "
+                       "K steps each reading the all-reduced energies back, D2H of its own particles; the two "
+                       "state copies are shared by the K steps"}
+    peak, peak_kind = measured_peak_hbm()
+    n = int(r["own"])
+    cells = cfg["mx"] * cfg["my"]
+    step_bytes = 96.0 * n + 60.0 * cells  # push 48 B + sort 48 B per particle, grid 60 B per cell
+    return {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (int64 fixed-point current, f64 energies)",
+        "data": "synthetic: seeded Philox GEM Harris sheet",
+        "config": {"workload": f"harris_{cfg['mx']}x{cfg['my']}_ppc{ld['ppc']}_yslabs",
+                   "grid": f"{cfg['mx']}x{cfg['my']}", "particles": n, "ppc_per_species": ld["ppc"],
+                   "rows_per_rank": args.slab_rows, "ghost_rows": lay.g, "ybc": "conducting", "xbc": "periodic",
+                   "seed": ld["seed"], "step": "push+fieldsolve+exchange+sort", "sort_every": 1,
+                   "l2": "inputs larger than L2 (particle state per rank about 2.5 GB FP32)",
+                   "parallelism": f"y-slabs x{ranks.world} (NCCL point-to-point ghost bands and rows)"},
+        "roofline": {"bound": "hbm", "step_frac": step_bytes / (r["ms"] / args.steps * 1e-3) / 1e9 / ranks.world / peak,
+                     "peak": peak, "unit": "GB/s", "peak_kind": peak_kind},
+        "energy": {"total": float(sum(r["energies"])), "gauss_residual": r["gauss"]},
+        "e2e": e2e,
+        "gpu_launches": r["launches"],
+        "clocks": clocks,
+    }
+
+
+class SelfTransport:
+    """One slab in one process (a single GPU): every exchange is with itself."""
+
+    def allreduce(self, values, op):
+        import numpy as np
+        return np.asarray(values, dtype=np.float64)
+
+    def exchange(self, slabs, outgoing):
+        from pbpic_b200.slab import InProcess
+        return InProcess().exchange(slabs, outgoing)
+
+
 # ---------------------------------------------------------------------- CPU
 def run_cpu_sample(workload_name, steps, seed_offset=0):
     """The oracle (OpenMP over all host threads) on a bounded sample of the
@@ -322,6 +569,38 @@ def run_cpu_sample(workload_name, steps, seed_offset=0):
     return dict(value=n * steps / dt, cores=nth, n=n, steps=steps, seconds=dt,
                 sample=f"{cfg['mx']}x{cfg['my']} cells, {ppc} particles/cell/species ({n} particles), {steps} steps "
                        "of push+fieldsolve+sort, FP64, OpenMP over all host threads")
+
+
+def run_cpu_full(workload_name, steps, warmup):
+    """The oracle (OpenMP over all host threads, FP64) on the whole workload:
+    `warmup` untimed steps, then `steps` timed steps of push + field solve +
+    sort, as the GPU arm runs them."""
+    from oracle import oracle as O
+    cfg, ld = workload(workload_name)
+    p, yee = O.load_plasma(cfg, ld)
+    o = O.Oracle(**cfg)
+    o.load_particles(p)
+    n = len(p)
+    del p
+    o.set_fields(yee)
+    nth = O.max_threads()
+    o.omp_countingsort(nth)
+
+    def one():
+        o.omp_pusher(nth)
+        o.fieldsolver()
+        o.omp_countingsort(nth)
+
+    for _ in range(warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    dt = time.perf_counter() - t0
+    o.close()
+    return dict(value=n * steps / dt, cores=nth, n=n, steps=steps, warmup=warmup, seconds=dt,
+                sample=f"the whole workload: {cfg['mx']}x{cfg['my']} cells, {n} particles, {warmup} untimed + "
+                       f"{steps} timed steps of push+fieldsolve+sort, FP64, OpenMP over all host threads")
 
 
 def run_cpu_single_f32(steps=3):
@@ -357,15 +636,12 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        steps = max(1, min(args.steps, 2))
-        for _ in range(max(0, min(args.warmup, 1))):
-            pass
-        r = run_cpu_sample(args.workload, steps)
+        r = run_cpu_full(args.workload, args.steps, args.warmup)
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": r["steps"], "warmup": 0, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+                "steps": r["steps"], "warmup": r["warmup"], "ms_per_step": 1e3 * r["seconds"] / r["steps"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic: seeded Philox Harris sheet",
-                "config": {"workload": args.workload, "sample": r["sample"]},
+                "data": "synthetic: seeded Philox " + workload_kind(args.workload),
+                "config": dict(workload_config(args.workload, r["n"]), sample=r["sample"]),
                 "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
                                  "sample": r["sample"], "host": host_cpu()},
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -374,6 +650,12 @@ def main():
 
     from pbpic_b200.replicas import Ranks
     ranks = Ranks("nccl")
+    if (world > 1 and not args.replicas) or args.slabs:
+        line = slab_line(args, ranks)
+        ranks.close()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     cfg, res, clocks, e2e, ens = run_gpu(args, ranks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -394,10 +676,10 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (int64 fixed-point current, f64 energies)", "data": "synthetic: seeded Philox GEM Harris sheet",
-        "config": {"workload": args.workload, "grid": f"{cfg['mx']}x{cfg['my']}", "particles": n,
-                   "step": "push+fieldsolve+sort", "sort_every": args.sort_every, "ybc": "conducting",
-                   "l2": "inputs larger than L2 (particle state 2.5 GB)", "parallelism": f"replicas x{world}"},
+        "dtype": "f32 (int64 fixed-point current, f64 energies)",
+        "data": "synthetic: seeded Philox " + workload_kind(args.workload),
+        "config": dict(workload_config(args.workload, n), step="push+fieldsolve+sort", sort_every=args.sort_every,
+                       parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": achieved_push, "peak": peak, "unit": "GB/s",
                      "frac": achieved_push / peak, "traffic": PUSH_DRAM_BYTES_PER_PARTICLE * n,
                      "kernel": "k_push<float,true,true,false,true>",
@@ -423,9 +705,10 @@ def main():
         line["energy"]["mixed_vs_fp64_total_energy_rel_err_max"] = float(rel.max())
     if e2e:
         line["e2e"] = {"value": world * e2e["n"] * e2e["K"] / e2e["seconds"], "unit": UNIT,
-                       "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                       "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"], "K": e2e["K"],
                        "what": "H2D of the initial reference particle records (pinned), K steps each with a D2H "
-                               "of the energies, D2H of the final particles"}
+                               "of the energies, D2H of the final particles; the two state copies are shared "
+                               "by the K steps, so the figure grows with K"}
     if ens and "error" in ens:
         line["ensemble"] = ens
     elif ens:

@@ -1,11 +1,12 @@
-"""Independent replicas, one process per GPU.
+"""Ranks of a multi-GPU run (one process per GPU) and independent replicas.
 
-The single-domain step does not shard in this library (the y-slab
-decomposition of the reference's MPI version is not built), so N GPUs run N
-independent replicas of a workload, each with its own seed. There is no
-data-path collective: ranks meet only at barriers and in the reduction of the
-timings (the slowest rank's time), and the whole-job throughput is
-N x particles x steps / that time (weak scaling).
+`Ranks` holds the process group, the barriers and the max-over-ranks
+reduction of the timings that every multi-GPU run uses. With replicas, N GPUs
+run N independent copies of a workload, each with its own seed, with no
+data-path collective: the whole-job throughput is N x particles x steps / the
+slowest rank's time (weak scaling). The batched ensemble is replicas only;
+the single-domain step shards as y slabs (slab.py, bench.py's default for
+N > 1).
 """
 import datetime
 import os
