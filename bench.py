@@ -54,6 +54,10 @@ def parse(argv=None):
     ap.add_argument("--sort-every", type=int, default=1)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=20)
+    ap.add_argument("--no-c5", action="store_true", help="skip the 4096x2048 Harris sheet (1.68 G particles)")
+    ap.add_argument("--c5-steps", type=int, default=10)
+    ap.add_argument("--c5-sub-steps", type=int, default=200,
+                    help="steps of the FP32-vs-FP64 comparison on the 1024x512 subsample of that sheet")
     ap.add_argument("--slabs", action="store_true",
                     help="run the y-slab decomposition also at one GPU (it is the default for N > 1)")
     ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of y slabs")
@@ -241,7 +245,13 @@ def run_gpu(args, ranks):
             ens = run_ensemble(args)
         except Exception as exc:  # reported in the line; the headline stands on its own
             ens = dict(error=f"{type(exc).__name__}: {exc}")
-    return cfg, results, clocks, e2e, ens
+    c5 = None
+    if not args.no_c5 and world == 1:
+        try:
+            c5 = run_c5(args, stream)
+        except Exception as exc:  # reported in the line; the headline stands on its own
+            c5 = dict(error=f"{type(exc).__name__}: {exc}")
+    return cfg, results, clocks, e2e, dict(ensemble=ens, c5=c5)
 
 
 def run_e2e(args, cfg, ld, stream, barrier, max_over_ranks):
@@ -277,6 +287,72 @@ def run_e2e(args, cfg, ld, stream, barrier, max_over_ranks):
         dt = time.perf_counter() - t0
     dt = max_over_ranks(dt)
     return dict(seconds=dt, n=n, K=K, h2d=n * 32 / K, d2h=32 + n * 32 / K)
+
+
+def timed_steps(s, stream, K):
+    """K steps (push, field solve, sort as separate calls) timed with CUDA
+    events on the handle's stream: total ms and the mean ms of each phase."""
+    import torch
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for k in range(K):
+        ev[k][0].record(stream)
+        s.pusher()
+        ev[k][1].record(stream)
+        s.fieldsolver()
+        ev[k][2].record(stream)
+        s.countingsort()
+        ev[k][3].record(stream)
+    end.record(stream)
+    torch.cuda.synchronize()
+    return (start.elapsed_time(end), float(np.mean([e[0].elapsed_time(e[1]) for e in ev])),
+            float(np.mean([e[1].elapsed_time(e[2]) for e in ev])), float(np.mean([e[2].elapsed_time(e[3]) for e in ev])))
+
+
+def run_c5(args, stream):
+    """The large Harris sheet: 4096 x 2048 cells of 0.05 d_i, 100 particles per
+    cell per species (1,677,721,600 particles, 40 GB of FP32 state, 114 GB
+    with the sort's second buffer and tables), mi/me = 100, nb = 0.1, guide
+    field 0.2, seed 4, FP32 mixed, sort every step: device-timed steps with
+    per-phase times. Its energy error: the FP32 mixed and FP64 plain forms
+    stepped side by side on a 1024 x 512 subsample of the same sheet (the same
+    cell size and physics), their largest relative total-energy difference."""
+    import pbpic_b200
+    from pbpic_b200 import configs
+    cfg, ld = configs.harris_c5()
+    n = pbpic_b200.Simulation(**cfg, precision="fp32", capacity=1).loader_count(**ld)
+    with pbpic_b200.Simulation(**cfg, precision="fp32", capacity=n, options=pbpic_b200.OPT_NO_AUTOSORT) as s:
+        s.set_stream(stream.cuda_stream)
+        s.init_plasma(**ld)
+        s.step(max(args.warmup, 3), sort_every=1)
+        s.synchronize()
+        l0 = pbpic_b200.kernel_launches()
+        total, tp, tf, ts = timed_steps(s, stream, args.c5_steps)
+        launches = pbpic_b200.kernel_launches() - l0
+        status = s.status()
+        gauss = s.gauss_residual()
+    K = args.c5_steps
+    sub_cfg, sub_ld = configs.harris(1024, 512, 100, seed=4, mime=100.0, nb=0.1, bguide=0.2, dx=0.05)
+    hist = {}
+    for prec in ("fp32", "fp64"):
+        m = pbpic_b200.Simulation(**sub_cfg, precision=prec, capacity=1).loader_count(**sub_ld)
+        with pbpic_b200.Simulation(**sub_cfg, precision=prec, capacity=m) as s:
+            s.set_stream(stream.cuda_stream)
+            s.init_plasma(**sub_ld)
+            s.step(args.c5_sub_steps, sort_every=1)
+            hist[prec] = s.energy_history().sum(axis=1)
+    rel = np.abs(hist["fp32"] - hist["fp64"]) / np.abs(hist["fp64"])
+    return {"workload": "harris_4096x2048_ppc100 (mi/me 100, nb 0.1, guide field 0.2, dx 0.05, seed 4)",
+            "particles": n, "steps": K, "ms_per_step": total / K, "value": n * K / (total * 1e-3), "unit": UNIT,
+            "phase_ms": {"push": tp, "fieldsolve": tf, "sort": ts},
+            "push_gbs": 48.0 * n / (tp * 1e-3) / 1e9, "sort_gbs_8B": 8.0 * n / (ts * 1e-3) / 1e9,
+            "gpu_launches": launches, "gauss_residual": gauss, "status": status,
+            "energy_error_subsample": {"grid": "1024x512", "steps": args.c5_sub_steps,
+                                       "mixed_vs_fp64_total_energy_rel_err_max": float(rel.max()),
+                                       "fp32_drift": float(abs(hist["fp32"][-1] / hist["fp32"][0] - 1.0)),
+                                       "fp64_drift": float(abs(hist["fp64"][-1] / hist["fp64"][0] - 1.0))}}
 
 
 def run_ensemble(args):
@@ -656,7 +732,8 @@ def main():
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
-    cfg, res, clocks, e2e, ens = run_gpu(args, ranks)
+    cfg, res, clocks, e2e, extra = run_gpu(args, ranks)
+    ens, c5 = extra["ensemble"], extra["c5"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_sample(args.workload, 4)
@@ -724,6 +801,10 @@ def main():
             "gpu_launches": {"batched": ens["launches_batch"], "per_instance": ens["launches_single"]},
             "step_frac_hbm": 96.0 * ens["n"] * ens["K"] / (ens["t_batch"] * 1e-3) / 1e9 / peak,
             "weibel_gauss_residual_max": ens["gauss"], "status": ens["status"]}
+    if c5:
+        if "push_gbs" in c5:
+            c5["push_frac"] = c5["push_gbs"] / peak
+        line["c5"] = c5
     if cpu:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
                                 "sample": cpu["sample"], "host": host_cpu(),

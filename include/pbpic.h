@@ -278,6 +278,19 @@ int pbpic_counting_sort_keys_static(const int32_t* keys_dev, int64_t n, int32_t 
  * Values keep the handle's precision, so pbpic_restart reproduces the state
  * exactly. */
 int pbpic_dump(pbpic_handle* h, const char* dir);
+/* Writes the reference's own HDF5 dump files into directory `dir`, with its
+ * file names, dataset names, element types (its `real` is 4 bytes) and
+ * shapes, so that the reference's readers (restart, python/ and idl/ plots)
+ * open them: particles.h5 (particlesinfo, pic2d.f90:1358-1560: dx dy ux uy uz
+ * grid q pid of length the capacity, the particles first, and nptlact),
+ * fields%05d.h5 for the current step (fieldsinfo, pic2d.f90:1625-1830: ex ey
+ * ez bx by bz dive jx jy jz rho num over (0:mx+1, 1:my+1)), spectra.h5
+ * (energyinfo, pic2d.f90:2034-2090: a group "%05d" per call so far with
+ * "spectra", and "ebins"; bins of de_electron / de_ion, nbins of them; 0
+ * selects 0.005, de_electron and 1000) and energy_tot.h5 ("tote"). Written by
+ * a self-contained HDF5 writer (no HDF5 library: superblock version 0,
+ * contiguous datasets). */
+int pbpic_dump_h5(pbpic_handle* h, const char* dir, double de_electron, double de_ion, int32_t nbins);
 /* Loads a dump into a handle created with the same mx, my, ybc and precision
  * and enough capacity, sets its time step and energy history, and sorts the
  * particles (stable, so a dump taken right after a sort continues bit for

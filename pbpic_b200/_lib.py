@@ -117,6 +117,7 @@ SIGNATURES = {
     "pbpic_field_cuts": [_P, _P, _I32, _P, _I32, _P],
     "pbpic_set_field_filters": [_P, _I32, ctypes.c_double, ctypes.c_double],
     "pbpic_dump": [_P, ctypes.c_char_p],
+    "pbpic_dump_h5": [_P, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, _I32],
     "pbpic_band_extract": [_P, _I32, _I32, _I32, _I32, _P, _I64, _PI64],
     "pbpic_band_keep": [_P, _I32, _I32],
     "pbpic_band_append": [_P, _P, _I64, _I32, _I32],

@@ -23,6 +23,7 @@
 #include "kernels_push_cells.cuh"
 #include "kernels_slab.cuh"
 #include "kernels_sort.cuh"
+#include "h5_writer.h"
 #include "npy_io.h"
 #include "pic_common.h"
 #include "pic_fields_init.h"
@@ -187,6 +188,10 @@ struct pbpic_handle {
   int32_t* band_scratch = nullptr;  // and their scan's chunk totals
   int32_t* colbuf = nullptr;        // sorted slab paths: per-column counts and starts (8 x (mx + 1))
   int32_t* colscan = nullptr;       // and their scans' chunk totals
+  // spectra written by pbpic_dump_h5 so far (time step, 2 x nbins counts): the
+  // reference's spectra.h5 gains one group per call, so every call rewrites it
+  // with all of them
+  std::vector<std::pair<int32_t, std::vector<int32_t>>> h5_spectra;
   std::vector<void*> allocs;
 };
 
@@ -2102,6 +2107,138 @@ int do_dump(pbpic_handle* h, const std::string& dir) {
   return PBPIC_OK;
 }
 
+// The reference's HDF5 dumps (particlesinfo pic2d.f90:1358-1380 and
+// 1400-1560, fieldsinfo 1625-1830, energyinfo 2034-2112), written with
+// h5_writer.h: root datasets, the reference's names and element types (its
+// `real` is 4 bytes), Fortran dimensions (a, b) stored as C order (b, a).
+template <class T, bool MIXED>
+int do_dump_h5(pbpic_handle* h, const std::string& dir, double de_e, double de_i, int nbins) {
+  if (!make_dir(dir)) return fail(PBPIC_EINVAL, "cannot create the dump directory " + dir);
+  const pbpic_config& c = h->cfg;
+  const int mx = c.mx, my = c.my;
+  const int64_t n = h->n;
+  std::string err;
+  using h5w::Dataset;
+  auto vec_writer = [](const void* p) {
+    return [p](FILE* f, uint64_t bytes) { return fwrite(p, 1, bytes, f) == bytes; };
+  };
+  // ---- particles.h5: dx dy ux uy uz (real), grid q pid (integer) of length
+  // the capacity, the particles first (zeros after them, unwritten in the
+  // reference), and nptlact (one entry per rank: one rank here)
+  std::vector<pbpic_particle_f32> rec((size_t)std::max<int64_t>(n, 1));
+  int64_t got = 0;
+  TRY(pbpic_store_particles_f32(h, rec.data(), n, &got));
+  const uint64_t cap = (uint64_t)std::max<int64_t>(h->cap, n);
+  std::vector<std::vector<uint32_t>> cols(8, std::vector<uint32_t>((size_t)cap, 0u));
+  for (int64_t i = 0; i < n; ++i) {
+    const pbpic_particle_f32& r = rec[i];
+    memcpy(&cols[0][i], &r.dx, 4);
+    memcpy(&cols[1][i], &r.dy, 4);
+    memcpy(&cols[2][i], &r.ux, 4);
+    memcpy(&cols[3][i], &r.uy, 4);
+    memcpy(&cols[4][i], &r.uz, 4);
+    memcpy(&cols[5][i], &r.grid, 4);
+    memcpy(&cols[6][i], &r.q, 4);
+    memcpy(&cols[7][i], &r.pid, 4);
+  }
+  const int32_t nptlact = (int32_t)n;
+  {
+    h5w::Group root;
+    const char* names[8] = {"dx", "dy", "ux", "uy", "uz", "grid", "q", "pid"};
+    for (int k = 0; k < 8; ++k)
+      root.datasets.push_back(Dataset{names[k], k < 5 ? h5w::FLOAT : h5w::INT, 4, {cap}, vec_writer(cols[k].data())});
+    root.datasets.push_back(Dataset{"nptlact", h5w::INT, 4, {1}, vec_writer(&nptlact)});
+    if (!h5w::write_file(dir + "/particles.h5", root, &err)) return fail(PBPIC_EINVAL, err);
+  }
+  // particle number per cell (numdensity, pic2d.f90:1343-1353)
+  std::vector<int32_t> num((size_t)mx * my, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t g = (int64_t)rec[i].grid - 1;
+    if (g >= 0 && g < (int64_t)mx * my) num[(size_t)g] += 1;
+  }
+  cols.clear();
+  rec.clear();
+  // ---- fields%05d.h5: emf(0:mx+1, 1:my+1) and denjr(0:mx+1, 1:my+1) as
+  // (my+1) x (mx+2): x ghosts 0 and mx+1 are the periodic copies of columns
+  // mx and 1; the last row is the top ghost row (periodic y: a copy of row 1)
+  const int64_t pe = plane_elems(h);
+  std::vector<double> f6((size_t)(6 * pe)), j4((size_t)(4 * pe));
+  TRY((do_store_fields<T, MIXED>(h, f6.data())));
+  TRY(do_store_denjr(h, j4.data()));
+  const int W = mx + 2, H = my + 1;
+  auto at = [&](const double* plane, int iref, int jref) {  // reference (iref, jref), 0..mx+1, 1..my+1
+    int i = iref - 1, j = jref - 1;
+    i = i < 0 ? i + mx : (i >= mx ? i - mx : i);
+    if (c.ybc == PBPIC_BC_PERIODIC && j == my) j = 0;
+    return plane[(size_t)i * h->S + j];
+  };
+  std::vector<std::vector<float>> fl(11, std::vector<float>((size_t)W * H));
+  std::vector<int32_t> numd((size_t)W * H, 0);
+  for (int jr = 1; jr <= my + 1; ++jr)
+    for (int ir = 0; ir <= mx + 1; ++ir) {
+      const size_t o = (size_t)(jr - 1) * W + ir;
+      for (int k = 0; k < 6; ++k) fl[k][o] = (float)at(f6.data() + (size_t)k * pe, ir, jr);
+      // dive (emf%dive): div E at the node, (ex(i,j) - ex(i-1,j))/dx + (ey(i,j) - ey(i,j-1))/dy
+      fl[6][o] = (float)((at(f6.data(), ir, jr) - at(f6.data(), ir - 1, jr)) / c.dx +
+                         (at(f6.data() + pe, ir, jr) - at(f6.data() + pe, ir, jr == 1 ? my : jr - 1)) / c.dy);
+      for (int k = 0; k < 4; ++k) fl[7 + k][o] = (float)at(j4.data() + (size_t)k * pe, ir, jr);
+      if (ir >= 1 && ir <= mx && jr <= my) numd[o] = num[(size_t)(ir - 1) * my + (jr - 1)];
+    }
+  {
+    h5w::Group root;
+    const char* names[11] = {"ex", "ey", "ez", "bx", "by", "bz", "dive", "jx", "jy", "jz", "rho"};
+    for (int k = 0; k < 11; ++k)
+      root.datasets.push_back(Dataset{names[k], h5w::FLOAT, 4, {(uint64_t)H, (uint64_t)W}, vec_writer(fl[k].data())});
+    root.datasets.push_back(Dataset{"num", h5w::INT, 4, {(uint64_t)H, (uint64_t)W}, vec_writer(numd.data())});
+    char name[32];
+    snprintf(name, sizeof(name), "/fields%05d.h5", h->itime);
+    if (!h5w::write_file(dir + name, root, &err)) return fail(PBPIC_EINVAL, err);
+  }
+  // ---- spectra.h5: one group "%05d" per dumped time step with "spectra"
+  // (integer, (2, nbins): electrons, ions), and "ebins" (real, bin upper edges)
+  std::vector<int64_t> sp((size_t)2 * nbins);
+  TRY(pbpic_energy_spectra(h, de_e, de_i, nbins, sp.data()));
+  std::vector<int32_t> spc((size_t)2 * nbins);
+  for (int b = 0; b < nbins; ++b) {
+    spc[(size_t)2 * b] = (int32_t)sp[(size_t)b];
+    spc[(size_t)2 * b + 1] = (int32_t)sp[(size_t)nbins + b];
+  }
+  auto same = std::find_if(h->h5_spectra.begin(), h->h5_spectra.end(),
+                           [&](const std::pair<int32_t, std::vector<int32_t>>& e) { return e.first == h->itime; });
+  if (same != h->h5_spectra.end()) same->second = spc;
+  else h->h5_spectra.push_back({h->itime, spc});
+  std::vector<float> ebins((size_t)2 * nbins);
+  for (int b = 0; b < nbins; ++b) {
+    ebins[(size_t)2 * b] = (float)((b + 1) * de_e);
+    ebins[(size_t)2 * b + 1] = (float)((b + 1) * de_i);
+  }
+  {
+    h5w::Group root;
+    for (const auto& e : h->h5_spectra) {
+      char gname[16];
+      snprintf(gname, sizeof(gname), "%05d", e.first);
+      h5w::Group g;
+      g.name = gname;
+      g.datasets.push_back(Dataset{"spectra", h5w::INT, 4, {(uint64_t)(e.second.size() / 2), 2}, vec_writer(e.second.data())});
+      root.groups.push_back(g);
+    }
+    root.datasets.push_back(Dataset{"ebins", h5w::FLOAT, 4, {(uint64_t)nbins, 2}, vec_writer(ebins.data())});
+    if (!h5w::write_file(dir + "/spectra.h5", root, &err)) return fail(PBPIC_EINVAL, err);
+  }
+  // ---- energy_tot.h5: tote, (4, ntime) energies of the steps so far
+  const int rows = h->itime + 1;
+  std::vector<double> hist((size_t)rows * 4);
+  CK(cudaMemcpyAsync(hist.data(), h->hist, hist.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  std::vector<float> tote(hist.begin(), hist.end());
+  {
+    h5w::Group root;
+    root.datasets.push_back(Dataset{"tote", h5w::FLOAT, 4, {(uint64_t)rows, 4}, vec_writer(tote.data())});
+    if (!h5w::write_file(dir + "/energy_tot.h5", root, &err)) return fail(PBPIC_EINVAL, err);
+  }
+  return PBPIC_OK;
+}
+
 template <class T, bool MIXED>
 int do_restart(pbpic_handle* h, const std::string& dir) {
   std::map<std::string, double> st;
@@ -2174,6 +2311,16 @@ int pbpic_dump(pbpic_handle* h, const char* dir) {
   TRY(check_handle(h));
   if (!dir) return fail(PBPIC_EINVAL, "null directory");
   return DISPATCH(h, do_dump, h, std::string(dir));
+}
+
+int pbpic_dump_h5(pbpic_handle* h, const char* dir, double de_electron, double de_ion, int32_t nbins) {
+  TRY(check_handle(h));
+  if (!dir) return fail(PBPIC_EINVAL, "null directory");
+  if (de_electron <= 0) de_electron = 0.005;
+  if (de_ion <= 0) de_ion = de_electron;
+  if (nbins <= 0) nbins = 1000;
+  if (nbins > 8192) return fail(PBPIC_EINVAL, "spectra take 1..8192 bins");
+  return DISPATCH(h, do_dump_h5, h, std::string(dir), de_electron, de_ion, (int)nbins);
 }
 
 int pbpic_restart(pbpic_handle* h, const char* dir) {

@@ -176,6 +176,12 @@ class Simulation:
         """Write the state as .npy files named like the reference's dump datasets."""
         L.check(self._lib.pbpic_dump(self._h, str(directory).encode()))
 
+    def dump_h5(self, directory, de_electron=0.0, de_ion=0.0, nbins=0):
+        """Write the reference's HDF5 dump files (particles.h5, fields%05d.h5,
+        spectra.h5 with one group per call, energy_tot.h5) into `directory`;
+        0 selects the default bins (0.005, de_electron, 1000)."""
+        L.check(self._lib.pbpic_dump_h5(self._h, str(directory).encode(), de_electron, de_ion, nbins))
+
     def restart(self, directory):
         """Load a dump written by dump() (same grid, boundary and precision)."""
         L.check(self._lib.pbpic_restart(self._h, str(directory).encode()))

@@ -80,3 +80,57 @@ def test_restart_rejects_another_grid(gpu_lib, tmp_path):
     with new_sim(cfg, ld, "fp64") as c:
         with pytest.raises(pbpic_b200.PbpicError):
             c.restart(tmp_path / "d")
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("kind", ["uniform", "harris"])
+def test_hdf5_dumps_hold_the_state(gpu_lib, tmp_path, precision, kind):
+    """pbpic_dump_h5 writes the reference's HDF5 files: particles.h5 (the
+    particle records, zeros up to the capacity, nptlact), fields%05d.h5 (E, B,
+    J, rho, div E and the particles per cell over the reference's index range
+    (0:mx+1, 1:my+1), as float32 / int32), spectra.h5 (a group per call) and
+    energy_tot.h5; read back with the test reader of the file format."""
+    from h5_reader import read
+
+    from pbpic_b200 import PARTICLE_F32
+    cfg, ld = case(kind)
+    mx, my = cfg["mx"], cfg["my"]
+    d = tmp_path / "h5"
+    with new_sim(cfg, ld, precision) as s:
+        s.init_plasma(**ld)
+        s.step(2, sort_every=1)
+        s.dump_h5(d, nbins=200)
+        s.step(3, sort_every=1)
+        s.dump_h5(d, nbins=200)
+        p32 = s.particles(PARTICLE_F32)
+        yee, jj, n = s.fields(), s.denjr(), s.num_particles()
+        hist, counts = s.energy_history(), s.cell_counts()
+        spect = s.energy_spectra(nbins=200)
+        cap = 2 * ld["ppc"] * mx * my
+    pf = read(str(d / "particles.h5"))
+    assert int(pf["nptlact"][0]) == n
+    for c in ("dx", "dy", "ux", "uy", "uz", "grid", "q", "pid"):
+        assert pf[c].shape == (cap,)
+        assert np.array_equal(pf[c][:n], p32[c]), c
+        assert not pf[c][n:].any()
+    ff = read(str(d / "fields00005.h5"))
+    assert (d / "fields00002.h5").exists()
+    ix = (np.arange(mx + 2) - 1) % mx  # reference column 0..mx+1 -> 0-based column
+    iy = np.arange(my + 1)             # reference row 1..my+1 -> 0-based row
+    if cfg["ybc"] == 0:
+        iy[my] = 0
+    for k, c in enumerate(("ex", "ey", "ez", "bx", "by", "bz")):
+        want = yee[k][ix][:, iy].T.astype(np.float32)
+        assert ff[c].shape == (my + 1, mx + 2) and np.array_equal(ff[c], want), c
+    for k, c in enumerate(("jx", "jy", "jz", "rho")):
+        assert np.array_equal(ff[c], jj[k][ix][:, iy].T.astype(np.float32)), c
+    num = np.zeros((my + 1, mx + 2), dtype=np.int32)
+    num[:my, 1:mx + 1] = counts.reshape(mx, my).T
+    assert np.array_equal(ff["num"], num)
+    assert ff["dive"].dtype == np.float32 and ff["dive"].shape == (my + 1, mx + 2)
+    sf = read(str(d / "spectra.h5"))
+    assert sorted(sf) == ["00002", "00005", "ebins"]
+    assert np.array_equal(sf["00005"]["spectra"], spect.T.astype(np.int32))
+    assert np.allclose(sf["ebins"][:, 0], 0.005 * np.arange(1, 201), rtol=1e-6)
+    tf = read(str(d / "energy_tot.h5"))
+    assert np.array_equal(tf["tote"], hist.astype(np.float32))
