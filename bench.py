@@ -33,11 +33,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy error"
-# DRAM bytes per particle of one k_push launch (read + write: the state read through the sort's
-# permutation, the permutation itself, the state written in cell order) from the ncu capture
-# summarised in profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to
-# the particles.
-PUSH_DRAM_BYTES_PER_PARTICLE = 61.0
+# DRAM bytes per particle of one launch of the mixed-form push as benchmarked (read + write: the
+# state read through the sort's permutation, the permutation itself, the state written in cell
+# order), from the ncu capture of the 512x256 sheet summarised in
+# profiles/k_push_cells_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to the
+# particles. None until that capture exists.
+PUSH_DRAM_BYTES_PER_PARTICLE = None
+PUSH_KERNEL = "k_push_cells<float,true,false,true>"
 UNIT = "particle-steps/s"
 
 
@@ -758,8 +760,9 @@ def main():
         "config": dict(workload_config(args.workload, n), step="push+fieldsolve+sort", sort_every=args.sort_every,
                        parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": achieved_push, "peak": peak, "unit": "GB/s",
-                     "frac": achieved_push / peak, "traffic": PUSH_DRAM_BYTES_PER_PARTICLE * n,
-                     "kernel": "k_push<float,true,true,false,true>",
+                     "frac": achieved_push / peak,
+                     "traffic": PUSH_DRAM_BYTES_PER_PARTICLE * n if PUSH_DRAM_BYTES_PER_PARTICLE else None,
+                     "kernel": PUSH_KERNEL,
                      "bytes_per_launch": bytes_push, "peak_kind": peak_kind,
                      "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": achieved_push / NOMINAL_HBM_GBS,
                      "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak},

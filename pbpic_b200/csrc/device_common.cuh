@@ -26,6 +26,12 @@ struct PushThreads {
   static constexpr int value = sizeof(T) == 4 ? PBPIC_PUSH_THREADS_FP32 : PBPIC_PUSH_THREADS_FP64;
 };
 
+// Mixed form: the per-cell gather records hold each field's bilinear
+// coefficients over the cell (1) or the cell's 4 nodes (0).
+#ifndef PBPIC_CELL_COEF
+#define PBPIC_CELL_COEF 1
+#endif
+
 // Current components (denjr record of pic2d.f90:65-67).
 enum { JX = 0, JY = 1, JZ = 2, RHO = 3 };
 

@@ -195,10 +195,11 @@ __global__ void k_nodes(FieldParams<T> a) {
   nodes_body(a, red, blockIdx.x, gridDim.x);
 }
 
-// Gather records of the mixed-form push from the node grid: cell (cx, cy) gets
-// its nodes (cx, cy), (cx, cy+1), (cx+1, cy), (cx+1, cy+1), each ex ey ez bx by
-// bz, as 6 contiguous 16-byte stores, so the push reads a cell's 4 nodes with 6
-// loads from one address instead of 8 from two.
+// Gather records of the mixed-form push from the node grid: cell (cx, cy)
+// gets, from its nodes (cx, cy), (cx, cy+1), (cx+1, cy), (cx+1, cy+1), the
+// bilinear coefficients (A, B, C, D) of each of ex ey ez bx by bz over the cell
+// (with PBPIC_CELL_COEF = 0 the 4 nodes themselves), as 6 contiguous 16-byte
+// stores, so the push reads a cell's gather data with 6 loads from one address.
 __device__ __forceinline__ void cell_records_body(const FieldParams<float>& a, int bid, int nblk) {
   const long long n = (long long)a.mx * a.my;
   for (long long c = bid * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)nblk * blockDim.x) {
@@ -208,12 +209,28 @@ __device__ __forceinline__ void cell_records_body(const FieldParams<float>& a, i
     const float4 p0 = g00[0], q0 = g00[1], p1 = g00[2], q1 = g00[3];  // nodes 00, 01: ex ey ez 0 | bx by bz 0
     const float4 p2 = g10[0], q2 = g10[1], p3 = g10[2], q3 = g10[3];  // nodes 10, 11
     float4* r = reinterpret_cast<float4*>(a.cg + c * 24);
+#if PBPIC_CELL_COEF
+    // per field: A = mean of the 4 nodes, B = x slope, C = y slope, D = twist
+    auto coef = [](float n00, float n01, float n10, float n11) {
+      const float sx0 = __fadd_rn(n00, n01), sx1 = __fadd_rn(n10, n11);
+      const float sy0 = __fadd_rn(n00, n10), sy1 = __fadd_rn(n01, n11);
+      return make_float4(__fmul_rn(0.25f, __fadd_rn(sx0, sx1)), __fmul_rn(0.5f, __fsub_rn(sx1, sx0)),
+                         __fmul_rn(0.5f, __fsub_rn(sy1, sy0)), __fsub_rn(__fsub_rn(n11, n10), __fsub_rn(n01, n00)));
+    };
+    r[0] = coef(p0.x, p1.x, p2.x, p3.x);
+    r[1] = coef(p0.y, p1.y, p2.y, p3.y);
+    r[2] = coef(p0.z, p1.z, p2.z, p3.z);
+    r[3] = coef(q0.x, q1.x, q2.x, q3.x);
+    r[4] = coef(q0.y, q1.y, q2.y, q3.y);
+    r[5] = coef(q0.z, q1.z, q2.z, q3.z);
+#else
     r[0] = make_float4(p0.x, p0.y, p0.z, q0.x);
     r[1] = make_float4(q0.y, q0.z, p1.x, p1.y);
     r[2] = make_float4(p1.z, q1.x, q1.y, q1.z);
     r[3] = make_float4(p2.x, p2.y, p2.z, q2.x);
     r[4] = make_float4(q2.y, q2.z, p3.x, p3.y);
     r[5] = make_float4(p3.z, q3.x, q3.y, q3.z);
+#endif
   }
 }
 

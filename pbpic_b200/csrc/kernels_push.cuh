@@ -95,6 +95,25 @@ __device__ __forceinline__ Node6<double> load_node(const double* g) {
   return Node6<double>{a.x, a.y, b.x, c.x, c.y, d.x};
 }
 
+// Mixed form: a cell's gather record (k_cell_records) holds, per field (ex ey
+// ez bx by bz, one aligned 16-byte group each), the bilinear coefficients
+// (A, B, C, D) of the field over the cell, f(x, y) = A + B x + C y + D x y for
+// the in-cell offsets x, y in [-1/2, 1/2): the same bilinear interpolation of
+// the 4 nodes as pic2d.f90:948-963, 3 FMAs per field. PBPIC_CELL_COEF = 0
+// (device_common.cuh) keeps the 4 nodes themselves instead.
+
+struct CellCoef {
+  float4 f[6];
+};
+__device__ __forceinline__ void load_coef(const float* r, CellCoef& c) {
+  const float4* q = reinterpret_cast<const float4*>(r);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) c.f[k] = __ldg(q + k);
+}
+__device__ __forceinline__ float coef_at(const float4& q, float x, float y) {
+  return __fmaf_rn(__fmaf_rn(q.w, x, q.z), y, __fmaf_rn(q.y, x, q.x));
+}
+
 // The 4 gather nodes of a cell from its record: n00, n01, n10, n11, each ex ey
 // ez bx by bz (6 aligned 16-byte loads from one address).
 __device__ __forceinline__ void load_cell(const float* r, Node6<float>& n00, Node6<float>& n01, Node6<float>& n10,
@@ -158,6 +177,10 @@ struct Pushed {
   int status;
 };
 
+template <class T, bool MIXED, bool COMPAT = true>
+__device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux, T puy,
+                                          T puz, T ex, T ey, T ez, T bx, T by, T bz, Pushed<T>& o);
+
 // Push of one particle whose gather nodes are n00 (ix,iy), n01 (ix,iy+1),
 // n10 (ix+1,iy), n11 (ix+1,iy+1). MIXED is only instantiated with T = float.
 // COMPAT = false compiles the step for a configuration without the compat
@@ -181,6 +204,24 @@ __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix,
   const T ex = PBD_GATHER(ex), ey = PBD_GATHER(ey), ez = PBD_GATHER(ez);
   const T bx = PBD_GATHER(bx), by = PBD_GATHER(by), bz = PBD_GATHER(bz);
 #undef PBD_GATHER
+  push_core<T, MIXED, COMPAT>(a, sp, ix, iy, px, py, pux, puy, puz, ex, ey, ez, bx, by, bz, o);
+}
+
+// Mixed form, from the cell's bilinear coefficients.
+template <bool COMPAT = true>
+__device__ __forceinline__ void push_one_coef(const PushParams<float>& a, int sp, int ix, int iy, float px, float py,
+                                              float pux, float puy, float puz, const CellCoef& c, Pushed<float>& o) {
+  push_core<float, true, COMPAT>(a, sp, ix, iy, px, py, pux, puy, puz, coef_at(c.f[0], px, py),
+                                 coef_at(c.f[1], px, py), coef_at(c.f[2], px, py), coef_at(c.f[3], px, py),
+                                 coef_at(c.f[4], px, py), coef_at(c.f[5], px, py), o);
+}
+
+// Everything after the gather: Boris, move, deposit terms, boundaries.
+template <class T, bool MIXED, bool COMPAT>
+__device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux, T puy,
+                                          T puz, T ex, T ey, T ez, T bx, T by, T bz, Pushed<T>& o) {
+  using A = M<T, MIXED>;
+  const T half = T(0.5), one = T(1);
   // Boris rotation, pic2d.f90:969-996
   const T c0 = sp ? a.c0[1] : a.c0[0], c1 = sp ? a.c1[1] : a.c1[0];
   const T umx = A::mad(c1, ex, pux), umy = A::mad(c1, ey, puy), umz = A::mad(c1, ez, puz);
@@ -615,6 +656,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     int first_key = -1;  // cell of this pass's finished first part (in `first`), or -1
     int cache_cell = -1;
     Node6<T> n00{}, n01{}, n10{}, n11{};
+    CellCoef cc;  // mixed form with coefficient records
     T pke_e = T(0), pke_i = T(0);  // this pass's kinetic energy, per species
 #pragma unroll 1
     for (int g = 0; g < G; ++g) {
@@ -685,7 +727,9 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
         const int cid = (ix << 16) | iy;
         if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
-          if constexpr (MIXED) {
+          if constexpr (MIXED && PBPIC_CELL_COEF) {
+            load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
+          } else if constexpr (MIXED) {
             load_cell(a.cg + ((long long)ix * a.my + iy) * 24, n00, n01, n10, n11);
           } else {  // FP64: from the node grid (its records took more registers than they saved)
             const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
@@ -698,7 +742,10 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           cache_cell = cid;
         }
         Pushed<T> o;
-        push_one<T, MIXED, COMPAT>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
+        if constexpr (MIXED && PBPIC_CELL_COEF)
+          push_one_coef<COMPAT>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], cc, o);
+        else
+          push_one<T, MIXED, COMPAT>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
         status |= o.status;
         const bool inwin = ix == ixt && iy >= y0 && iy < y1;
         const bool cross = o.dcx != 0 || o.dcy != 0;

@@ -10,8 +10,8 @@
 // coalesced 128-byte access per array (through the sort's permutation the
 // elements of a cell are almost consecutive), and every lane of the warp is in
 // the same cell:
-//   - the cell's gather nodes are loaded once per cell (one broadcast record)
-//     and stay in registers;
+//   - the cell's gather record (bilinear coefficients of the 6 fields) is
+//     loaded once per cell (one broadcast record) and stays in registers;
 //   - each lane sums the 17-value deposit stencil of its particles in
 //     registers; at the end of the cell one transposing reduction over the
 //     warp (five shuffle rounds that halve the values a lane holds) leaves
@@ -159,7 +159,10 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
     const int key = iy - y0;
     const uint32_t cw0 = cw_make(ixt, iy, 0);
     Node6<T> n00, n01, n10, n11;
-    if constexpr (MIXED) {
+    CellCoef cc;
+    if constexpr (MIXED && PBPIC_CELL_COEF) {
+      load_coef(a.cg + c * 24, cc);
+    } else if constexpr (MIXED) {
       load_cell(a.cg + c * 24, n00, n01, n10, n11);
     } else {
       const T* g00 = a.ng + ((long long)ixt * (a.my + 1) + iy) * 8;
@@ -206,7 +209,10 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
           ouz[p] = puz;
         } else {
           Pushed<T> o;
-          push_one<T, MIXED, COMPAT>(a, sp, ixt, iy, px, py, pux, puy, puz, n00, n01, n10, n11, o);
+          if constexpr (MIXED && PBPIC_CELL_COEF)
+            push_one_coef<COMPAT>(a, sp, ixt, iy, px, py, pux, puy, puz, cc, o);
+          else
+            push_one<T, MIXED, COMPAT>(a, sp, ixt, iy, px, py, pux, puy, puz, n00, n01, n10, n11, o);
           status |= o.status;
           const bool cross = o.dcx != 0 || o.dcy != 0;
           if (cross) {

@@ -28,7 +28,7 @@ module pbpic_gpu
     integer(c_int32_t), parameter :: PBPIC_BC_PERIODIC = 0, PBPIC_BC_CONDUCTING = 1
     integer(c_int32_t), parameter :: PBPIC_FP64_PLAIN = 0, PBPIC_FP32_MIXED = 1
     integer(c_int32_t), parameter :: PBPIC_COMPAT_BORIS = 1, PBPIC_COMPAT_FOLD = 2, PBPIC_COMPAT_RHO = 4
-    integer(c_int32_t), parameter :: PBPIC_OPT_NO_AUTOSORT = 1
+    integer(c_int32_t), parameter :: PBPIC_OPT_NO_AUTOSORT = 1, PBPIC_OPT_EXACT_FP64 = 2
     integer(c_int32_t), parameter :: PBPIC_FILTER_MARDER = 1, PBPIC_FILTER_CERENKOV = 2
     integer(c_int32_t), parameter :: PBPIC_LOAD_UNIFORM = 0, PBPIC_LOAD_HARRIS = 1, PBPIC_LOAD_TWO_STREAM = 2, &
                                      PBPIC_LOAD_WEIBEL = 3, PBPIC_LOAD_DOUBLE_HARRIS = 4
@@ -159,6 +159,15 @@ module pbpic_gpu
             import :: c_int, c_ptr, c_char
             type(c_ptr), value :: h
             character(kind=c_char), intent(in) :: dir(*)
+            integer(c_int) :: ierr
+        end function
+        ! the reference's own HDF5 files: particles.h5, fields%05d.h5, spectra.h5, energy_tot.h5
+        function pbpic_dump_h5(h, dir, de_electron, de_ion, nbins) bind(c, name="pbpic_dump_h5") result(ierr)
+            import :: c_int, c_ptr, c_char, c_double, c_int32_t
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: dir(*)
+            real(c_double), value :: de_electron, de_ion
+            integer(c_int32_t), value :: nbins
             integer(c_int) :: ierr
         end function
         function pbpic_restart(h, dir) bind(c, name="pbpic_restart") result(ierr)
