@@ -28,6 +28,15 @@
 // unchanged and STATUS_UNSORTED is set. The handle only runs this kernel on
 // particles sorted by its own counting sort.
 //
+// With PushParams::rankw the kernel also ranks every particle for the fused
+// counting sort: its direction (the window bin of its new cell relative to its
+// old cell, 9 values) and its rank among the particles of its cell with that
+// direction in position order (a match over the warp's lanes and a running
+// count per direction), as a rank word per position, and each row's count per
+// direction. The particles landing in a bin before a given one are then those
+// of earlier rows with the matching direction (at most 3 rows) plus its rank,
+// which k_fused_perm_rw turns into the sorted slot with a few additions.
+//
 // Sums: the lanes add their particles in sorted order, the reduction adds in a
 // fixed lane pattern, and the window holds integers in the mixed form, so the
 // mixed form's result does not depend on timing (bit-reproducible run to run).
@@ -40,6 +49,11 @@ namespace pbd {
 // library with k_push alone, for comparison).
 #ifndef PBPIC_PUSH_CELLS
 #define PBPIC_PUSH_CELLS 1
+#endif
+// The per-cell push writes rank words for the fused sort (0: the sort ranks
+// the pushed cell words itself, k_fused_perm).
+#ifndef PBPIC_PUSH_RANKS
+#define PBPIC_PUSH_RANKS 1
 #endif
 #ifndef PBPIC_CPUSH_THREADS
 #define PBPIC_CPUSH_THREADS 128
@@ -109,6 +123,7 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
   __shared__ int next_row;
+  __shared__ int dcount[PBPIC_CPUSH_THREADS / 32][16];  // rank words: the warp's running counts per direction
   const int t = blockIdx.x;
   const int TY = a.tile_rows, WR = TY + 3, NB = 3 * (TY + 2);
   Acc* win = reinterpret_cast<Acc*>(smem_raw);
@@ -176,9 +191,15 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
 #pragma unroll
     for (int k = 0; k < 17; ++k) acc[k] = T(0);
     T pke_e = T(0), pke_i = T(0);
+    const int w = threadIdx.x >> 5;
+    if (a.rankw) {
+      if (lane < 16) dcount[w][lane] = 0;
+      __syncwarp();
+    }
 #pragma unroll 1
     for (int q = pbeg; q < pend; q += 32) {
       const int p = q + (int)lane;
+      int dir = 15;  // rank words: this lane's direction (15: no particle)
       if (p < pend) {
         const int e = GATHER ? __ldg(a.src + p) : p;
         uint32_t wrd;
@@ -201,6 +222,7 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
         const int sp = cw_sp(wrd);
         if ((wrd & 0x7fffffffu) != cw0) {  // not this cell's particle: left as it is
           status |= 4;
+          dir = 4;  // ranked with this cell's particles, where its count is
           ocell[p] = wrd;
           odx[p] = px;
           ody[p] = py;
@@ -234,6 +256,7 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
               atomicAdd(&hist[b], 1);
               atomicAdd(&hist[bo], -1);
             }
+            dir = (b / (TY + 2)) * 3 + (b % (TY + 2) - key);
             // second zig-zag segment, attached to the new cell
             const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
             const int b0 = (JX * 4 + wx) * WR + wy, b1 = (JY * 4 + wx) * WR + wy;
@@ -291,6 +314,7 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
           acc[16] += o.e[15];
           if (sp) pke_e += o.ke;
           else pke_i += o.ke;
+          if (!cross) dir = 4;  // stays: window column 1, row key + 1
           ocell[p] = o.cw;
           odx[p] = o.dx;
           ody[p] = o.dy;
@@ -300,7 +324,20 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
         }
         if (GATHER && a.pid_o) a.pid_o[p] = __ldg(a.pid_i + e);
       }
+      if (a.rankw) {  // stable rank among this cell's particles of the same direction
+        const unsigned peers = __match_any_sync(FULL, dir);
+        const int before = dir < 9 ? dcount[w][dir] : 0;
+        __syncwarp();
+        if (dir < 9 && (peers & lanemask_lt()) == 0) dcount[w][dir] = before + __popc(peers);
+        __syncwarp();
+        if (p < pend) {
+          const int r = before + __popc(peers & lanemask_lt());
+          if (r >= (1 << 22)) status |= 1;  // a cell of more than 4 M particles
+          a.rankw[p] = (key << 26) | ((dir & 15) << 22) | (r & 0x3fffff);
+        }
+      }
     }
+    if (a.rankw && lane < 9) a.ctab[((long long)t * TY + key) * 9 + lane] = dcount[w][lane];
     ke_e += (double)pke_e;
     ke_i += (double)pke_i;
     const T v = warp_reduce17(acc, lane);

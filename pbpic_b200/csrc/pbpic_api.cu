@@ -170,6 +170,13 @@ struct pbpic_handle {
   // particle arrays applies it first (materialize).
   int32_t* perm = nullptr;
   bool lazy = false;
+  // The per-cell push's ranking for the fused sort (kernels_push_cells.cuh):
+  // a rank word per position and per tile the rows' counts per direction;
+  // ranks_valid while they belong to the last push.
+  int32_t* rankw = nullptr;
+  int32_t* ctab = nullptr;
+  int ctab_tiles = 0;
+  bool ranks_valid = false;
   size_t push_optin = 0;    // dynamic shared memory the plain form's k_push may take
   int nb = 0;               // window bins per tile, 3*(TY+2)
   int tile_cap = 0;         // tiles the per-tile arrays hold
@@ -319,6 +326,8 @@ PushParams<T> push_params(pbpic_handle* h) {
   p.dx_o = p.dy_o = p.ux_o = p.uy_o = p.uz_o = nullptr;
   p.pid_i = nullptr;
   p.pid_o = nullptr;
+  p.rankw = nullptr;
+  p.ctab = nullptr;
   const T dt = (T)c.dt, mime = (T)c.mime, cva = (T)c.cva, dx = (T)c.dx, dy = (T)c.dy;
   for (int s = 0; s < 2; ++s) {
     const T q = s == 0 ? T(1) : T(-1);
@@ -497,6 +506,7 @@ int do_sort(pbpic_handle* h) {
   CKLAUNCH("k_tile_off");
   h->sorted = true;
   h->hist_valid = false;
+  h->ranks_valid = false;
   return PBPIC_OK;
 }
 
@@ -518,6 +528,21 @@ int do_push(pbpic_handle* h) {
   // sorted input: one warp per cell (kernels_push_cells.cuh); smem: window, histogram, crossers' windows
   const int ct = PBPIC_CPUSH_THREADS;
   const size_t csmem = push_cells_smem_bytes(h->TY, MIXED);
+  h->ranks_valid = false;
+  if (PBPIC_PUSH_CELLS && PBPIC_PUSH_RANKS && hist && h->n > 0) {  // the push ranks the particles for the sort
+    if (!h->rankw) TRY(dalloc(h, (void**)&h->rankw, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
+    if (h->ctab_tiles < h->ntiles) {
+      if (h->ctab) {
+        cudaFree(h->ctab);
+        h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), (void*)h->ctab));
+        h->ctab = nullptr;
+      }
+      TRY(dalloc(h, (void**)&h->ctab, (size_t)h->ntiles * 64 * 9 * 4));
+      h->ctab_tiles = h->ntiles;
+    }
+    p.rankw = h->rankw;
+    p.ctab = h->ctab;
+  }
   // the compat instances also carry the plain form's exact-order arithmetic
   const bool compat = h->cfg.compat != 0 || (!MIXED && (h->cfg.options & PBPIC_OPT_EXACT_FP64));
   if (h->lazy) {  // read through the sort's permutation, write in cell order to the other buffer
@@ -551,6 +576,7 @@ int do_push(pbpic_handle* h) {
   k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
   CKLAUNCH("k_energy_row");
   h->hist_valid = hist;
+  h->ranks_valid = p.rankw != nullptr;
   h->sorted = false;
   if (autosort) TRY((do_fused_sort<T, MIXED>(h)));
   return PBPIC_OK;
@@ -597,8 +623,14 @@ int do_fused_sort(pbpic_handle* h) {
   if (n > 0) {  // the sorted order as a permutation; the particle data stay in place
     if (!h->perm) TRY(dalloc(h, &h->perm, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
     sp.perm = h->perm;
-    k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp);
-    CKLAUNCH("k_fused_perm");
+    if (h->ranks_valid && h->TY <= 64) {
+      RankParams rp{h->TY, h->nb, h->tile_off, h->tbase, h->rankw, h->ctab, h->perm};
+      k_fused_perm_rw<<<h->ntiles, 256, 0, s>>>(rp);
+      CKLAUNCH("k_fused_perm_rw");
+    } else {
+      k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp);
+      CKLAUNCH("k_fused_perm");
+    }
     h->lazy = true;
   }
   k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, h->cfg.my,
@@ -606,6 +638,7 @@ int do_fused_sort(pbpic_handle* h) {
   CKLAUNCH("k_tile_off");
   h->sorted = true;
   h->hist_valid = false;
+  h->ranks_valid = false;
   return PBPIC_OK;
 }
 
@@ -2540,6 +2573,7 @@ int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_
   CKLAUNCH("k_tile_off");
   h->sorted = true;
   h->hist_valid = false;
+  h->ranks_valid = false;
   return PBPIC_OK;
 }
 
