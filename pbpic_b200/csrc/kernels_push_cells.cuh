@@ -170,7 +170,10 @@ __global__ void __launch_bounds__(PBPIC_CPUSH_THREADS, MIXED ? PBPIC_CPUSH_MINBL
     if (iy >= y1) break;
     const long long c = cbase + iy;
     const int pbeg = a.cell_off[c], pend = a.cell_off[c + 1];
-    if (pbeg >= pend) continue;
+    if (pbeg >= pend) {  // an empty row sends nothing anywhere
+      if (a.rankw && lane < 9) a.ctab[((long long)t * TY + (iy - y0)) * 9 + lane] = 0;
+      continue;
+    }
     const int key = iy - y0;
     const uint32_t cw0 = cw_make(ixt, iy, 0);
     Node6<T> n00, n01, n10, n11;

@@ -513,6 +513,8 @@ int do_sort(pbpic_handle* h) {
 template <class T, bool MIXED>
 int do_push(pbpic_handle* h) {
   const bool autosort = !(h->cfg.options & PBPIC_OPT_NO_AUTOSORT) && h->fused_ok;
+  // the per-cell push for sorted input, unless the handle asks for the tile push
+  const bool cells = PBPIC_PUSH_CELLS && !(h->cfg.options & PBPIC_OPT_TILE_PUSH);
   if (autosort && !h->sorted) TRY((do_sort<T, MIXED>(h)));
   cudaStream_t s = h->stream;
   TRY(ensure_hist(h, h->itime + 2));
@@ -529,7 +531,7 @@ int do_push(pbpic_handle* h) {
   const int ct = PBPIC_CPUSH_THREADS;
   const size_t csmem = push_cells_smem_bytes(h->TY, MIXED);
   h->ranks_valid = false;
-  if (PBPIC_PUSH_CELLS && PBPIC_PUSH_RANKS && hist && h->n > 0) {  // the push ranks the particles for the sort
+  if (cells && PBPIC_PUSH_RANKS && hist && h->n > 0) {  // the push ranks the particles for the sort
     if (!h->rankw) TRY(dalloc(h, (void**)&h->rankw, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
     if (h->ctab_tiles < h->ntiles) {
       if (h->ctab) {
@@ -557,16 +559,16 @@ int do_push(pbpic_handle* h) {
     p.uz_o = P<T>(h, o, 4);
     p.pid_i = h->pid[h->cur];
     p.pid_o = h->pid[o];
-    if (PBPIC_PUSH_CELLS && !compat) k_push_cells<T, MIXED, false, true><<<h->ntiles, ct, csmem, s>>>(p);
-    else if (PBPIC_PUSH_CELLS) k_push_cells<T, MIXED, true, true><<<h->ntiles, ct, csmem, s>>>(p);
+    if (cells && !compat) k_push_cells<T, MIXED, false, true><<<h->ntiles, ct, csmem, s>>>(p);
+    else if (cells) k_push_cells<T, MIXED, true, true><<<h->ntiles, ct, csmem, s>>>(p);
     else if (!compat) k_push<T, MIXED, true, false, true><<<h->ntiles, nt, smem, s>>>(p);
     else k_push<T, MIXED, true, true, true><<<h->ntiles, nt, smem, s>>>(p);
     CKLAUNCH("k_push");
     h->cur = o;
     h->lazy = false;
   } else {
-    if (PBPIC_PUSH_CELLS && hist && !compat) k_push_cells<T, MIXED, false, false><<<h->ntiles, ct, csmem, s>>>(p);
-    else if (PBPIC_PUSH_CELLS && hist) k_push_cells<T, MIXED, true, false><<<h->ntiles, ct, csmem, s>>>(p);
+    if (cells && hist && !compat) k_push_cells<T, MIXED, false, false><<<h->ntiles, ct, csmem, s>>>(p);
+    else if (cells && hist) k_push_cells<T, MIXED, true, false><<<h->ntiles, ct, csmem, s>>>(p);
     else if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
     else if (hist) k_push<T, MIXED, true, true><<<h->ntiles, nt, smem, s>>>(p);
     else if (!compat) k_push<T, MIXED, false, false><<<h->ntiles, nt, smem, s>>>(p);
@@ -957,7 +959,8 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
     return fail(PBPIC_EINVAL, "unknown precision");
   if (c.capacity < 0 || c.capacity > 0x7fffff00ll) return fail(PBPIC_EINVAL, "capacity must be in [0, 2^31)");
   if (c.compat & ~7) return fail(PBPIC_EINVAL, "unknown compat bits");
-  if (c.options & ~(PBPIC_OPT_NO_AUTOSORT | PBPIC_OPT_EXACT_FP64)) return fail(PBPIC_EINVAL, "unknown option bits");
+  if (c.options & ~(PBPIC_OPT_NO_AUTOSORT | PBPIC_OPT_EXACT_FP64 | PBPIC_OPT_TILE_PUSH))
+    return fail(PBPIC_EINVAL, "unknown option bits");
   const double cfl = c.cva * c.dt * sqrt(1.0 / (c.dx * c.dx) + 1.0 / (c.dy * c.dy));
   if (!(cfl < 1.0)) return fail(PBPIC_EINVAL, "time step violates the CFL condition c*dt*sqrt(1/dx^2+1/dy^2) < 1");
   if (c.cva * c.dt / std::min(c.dx, c.dy) >= 1.0)
