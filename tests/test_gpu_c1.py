@@ -96,7 +96,7 @@ def test_c1_sort_and_step1_match_oracle(gpu_lib, oracle_mod, c1):
 
         # the step's sort: the stable counting sort of the step's input order
         # (g0's order) by the new cells, done by the oracle
-        pos = np.empty(n, dtype=np.int64)
+        pos = np.empty(int(g0["pid"].max()) + 1, dtype=np.int64)
         pos[g0["pid"]] = np.arange(n)
         in_order = o1[np.argsort(pos[o1["pid"]], kind="stable")]
         o2 = oracle_mod.Oracle(**cfg)
