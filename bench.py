@@ -36,10 +36,9 @@ METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy 
 # DRAM bytes per particle of one launch of the mixed-form push as benchmarked (read + write: the
 # state read through the sort's permutation, the permutation itself, the state written in cell
 # order), from the ncu capture of the 512x256 sheet summarised in
-# profiles/k_push_cells_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to the
-# particles. None until that capture exists.
+# profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to the particles.
 PUSH_DRAM_BYTES_PER_PARTICLE = None
-PUSH_KERNEL = "k_push_cells<float,true,false,true>"
+PUSH_KERNEL = "k_push<float,true,true,false,true>"
 UNIT = "particle-steps/s"
 
 

@@ -85,12 +85,6 @@ typedef struct pbpic_config {
  * state agrees with that evaluation to a few ulp (1e-15 relative), faster.
  * Any compat switch implies it. */
 #define PBPIC_OPT_EXACT_FP64 2
-/* The push of sorted particles runs the per-thread tile kernel (each thread
- * takes consecutive particles, the lanes sharing a cell sum their stencils in
- * lane order), the arithmetic of the batched form, instead of the default
- * one-warp-per-cell kernel: a handle stepped with it matches a batched domain
- * with the same tile rows bit for bit. */
-#define PBPIC_OPT_TILE_PUSH 4
 
 /* The reference's `type particle` (pic2d.f90:47-50): 32 bytes. grid is the
  * 1-based cell my*(ix-1)+iy (y fastest), dx, dy the offset from the cell

@@ -23,7 +23,6 @@ LOAD_UNIFORM, LOAD_HARRIS, LOAD_TWO_STREAM, LOAD_WEIBEL, LOAD_DOUBLE_HARRIS = 0,
 FILTER_MARDER, FILTER_CERENKOV = 1, 2
 OPT_NO_AUTOSORT = 1
 OPT_EXACT_FP64 = 2
-OPT_TILE_PUSH = 4
 
 
 class Config(ctypes.Structure):

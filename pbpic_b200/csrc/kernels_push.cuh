@@ -73,13 +73,6 @@ struct PushParams {
   T *dx_o, *dy_o, *ux_o, *uy_o, *uz_o;
   const int32_t* pid_i;  // tracked ids, moved with the particles (null: none)
   int32_t* pid_o;
-  // k_push_cells only (null: not written): per sorted position the particle's
-  // rank word (tile row << 26 | direction << 22 | rank among the particles of
-  // its cell that move in that direction, in position order), and per tile the
-  // counts of each row's particles per direction ([ntiles][tile_rows][9]);
-  // direction = window column (0..2) * 3 + (window row - tile row) (0..2).
-  int32_t* rankw;
-  int32_t* ctab;
   T c0[2], c1[2], ms[2], qx[2], qy[2], q[2];  // per species: 0 ion, 1 electron
   T dtcva, idx, idy, cva;
   double* ke_part;  // [ntiles][2]: electron, ion kinetic energy of the tile

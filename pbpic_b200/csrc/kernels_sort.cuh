@@ -515,45 +515,6 @@ __global__ void __launch_bounds__(256) k_fused_perm(ScatterParams<T> a) {
   perm_tile(a, blockIdx.x, sm);
 }
 
-// The permutation from the push's rank words (k_push_cells with rankw): a
-// particle at position p of tile t in row `key` with direction `dir` and rank
-// r lands in window bin b = (dir / 3) * (ty + 2) + key + dir % 3; the tile's
-// particles in b before it are those of the rows before `key` that move into b
-// (rows by - 2 .. by with the matching direction, whose counts are ctab) and
-// the r of its own row, so its slot is base[t][b] + those counts + r. The
-// same stable order as k_fused_perm (array order within each bin).
-struct RankParams {
-  int ty, nb;
-  const int32_t* tile_off;
-  const int32_t* base;   // [ntiles][nb]
-  const int32_t* rankw;  // per position
-  const int32_t* ctab;   // [ntiles][ty][9]
-  int32_t* perm;
-};
-
-static __global__ void __launch_bounds__(256) k_fused_perm_rw(RankParams a) {
-  __shared__ int32_t ct[64 * 9];
-  __shared__ int32_t sb[SC_MAXNB];
-  const int t = blockIdx.x;
-  const int TY = a.ty;
-  for (int e = threadIdx.x; e < TY * 9; e += blockDim.x) ct[e] = a.ctab[(int64_t)t * TY * 9 + e];
-  for (int b = threadIdx.x; b < a.nb; b += blockDim.x) sb[b] = a.base[(int64_t)t * a.nb + b];
-  __syncthreads();
-  const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
-  for (int p = pbeg + threadIdx.x; p < pend; p += blockDim.x) {
-    const int32_t wd = a.rankw[p];
-    const int key = (wd >> 26) & 63, dir = (wd >> 22) & 15, r = wd & 0x3fffff;
-    const int bx = dir / 3, by = key + dir % 3;
-    int before = 0;
-#pragma unroll
-    for (int d = 2; d >= 0; --d) {  // row by - d moving d rows up into bin (bx, by)
-      const int rho = by - d;
-      if (rho >= 0 && rho < key) before += ct[rho * 9 + bx * 3 + d];
-    }
-    a.perm[(int64_t)sb[bx * (TY + 2) + by] + before + r] = p;
-  }
-}
-
 // The identity permutation: arrays already in cell order, read through perm.
 static __global__ void k_iota(int32_t* perm, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

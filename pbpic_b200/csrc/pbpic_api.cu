@@ -20,7 +20,6 @@
 #include "kernels_field.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_push.cuh"
-#include "kernels_push_cells.cuh"
 #include "kernels_slab.cuh"
 #include "kernels_sort.cuh"
 #include "h5_writer.h"
@@ -170,13 +169,6 @@ struct pbpic_handle {
   // particle arrays applies it first (materialize).
   int32_t* perm = nullptr;
   bool lazy = false;
-  // The per-cell push's ranking for the fused sort (kernels_push_cells.cuh):
-  // a rank word per position and per tile the rows' counts per direction;
-  // ranks_valid while they belong to the last push.
-  int32_t* rankw = nullptr;
-  int32_t* ctab = nullptr;
-  int ctab_tiles = 0;
-  bool ranks_valid = false;
   size_t push_optin = 0;    // dynamic shared memory the plain form's k_push may take
   int nb = 0;               // window bins per tile, 3*(TY+2)
   int tile_cap = 0;         // tiles the per-tile arrays hold
@@ -234,13 +226,6 @@ int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
 size_t push_smem_bytes(int ty, bool mixed) {
   if (!mixed) return push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * sizeof(double);
   return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4;
-}
-
-// Dynamic shared memory of k_push_cells: the window (16 planes of ty+3 8-byte
-// sums), the new-cell histogram and, in the mixed form, the crossers' split
-// 32-bit windows.
-size_t push_cells_smem_bytes(int ty, bool mixed) {
-  return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (mixed ? (size_t)16 * (ty + 3) * 4 : 0);
 }
 
 // Lets the plain form's k_push instantiations take more than 48 KB of shared
@@ -326,8 +311,6 @@ PushParams<T> push_params(pbpic_handle* h) {
   p.dx_o = p.dy_o = p.ux_o = p.uy_o = p.uz_o = nullptr;
   p.pid_i = nullptr;
   p.pid_o = nullptr;
-  p.rankw = nullptr;
-  p.ctab = nullptr;
   const T dt = (T)c.dt, mime = (T)c.mime, cva = (T)c.cva, dx = (T)c.dx, dy = (T)c.dy;
   for (int s = 0; s < 2; ++s) {
     const T q = s == 0 ? T(1) : T(-1);
@@ -506,15 +489,12 @@ int do_sort(pbpic_handle* h) {
   CKLAUNCH("k_tile_off");
   h->sorted = true;
   h->hist_valid = false;
-  h->ranks_valid = false;
   return PBPIC_OK;
 }
 
 template <class T, bool MIXED>
 int do_push(pbpic_handle* h) {
   const bool autosort = !(h->cfg.options & PBPIC_OPT_NO_AUTOSORT) && h->fused_ok;
-  // the per-cell push for sorted input, unless the handle asks for the tile push
-  const bool cells = PBPIC_PUSH_CELLS && !(h->cfg.options & PBPIC_OPT_TILE_PUSH);
   if (autosort && !h->sorted) TRY((do_sort<T, MIXED>(h)));
   cudaStream_t s = h->stream;
   TRY(ensure_hist(h, h->itime + 2));
@@ -527,24 +507,6 @@ int do_push(pbpic_handle* h) {
   if (hist && !p.cell_off) return fail(PBPIC_EINVAL, "k_push: counting from the cell offsets needs them");
   if (MIXED && !p.cg) return fail(PBPIC_ESTATE, "k_push: no per-cell gather records");
   const int nt = PushThreads<T>::value;
-  // sorted input: one warp per cell (kernels_push_cells.cuh); smem: window, histogram, crossers' windows
-  const int ct = PBPIC_CPUSH_THREADS;
-  const size_t csmem = push_cells_smem_bytes(h->TY, MIXED);
-  h->ranks_valid = false;
-  if (cells && PBPIC_PUSH_RANKS && hist && h->n > 0) {  // the push ranks the particles for the sort
-    if (!h->rankw) TRY(dalloc(h, (void**)&h->rankw, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
-    if (h->ctab_tiles < h->ntiles) {
-      if (h->ctab) {
-        cudaFree(h->ctab);
-        h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), (void*)h->ctab));
-        h->ctab = nullptr;
-      }
-      TRY(dalloc(h, (void**)&h->ctab, (size_t)h->ntiles * 64 * 9 * 4));
-      h->ctab_tiles = h->ntiles;
-    }
-    p.rankw = h->rankw;
-    p.ctab = h->ctab;
-  }
   // the compat instances also carry the plain form's exact-order arithmetic
   const bool compat = h->cfg.compat != 0 || (!MIXED && (h->cfg.options & PBPIC_OPT_EXACT_FP64));
   if (h->lazy) {  // read through the sort's permutation, write in cell order to the other buffer
@@ -559,17 +521,13 @@ int do_push(pbpic_handle* h) {
     p.uz_o = P<T>(h, o, 4);
     p.pid_i = h->pid[h->cur];
     p.pid_o = h->pid[o];
-    if (cells && !compat) k_push_cells<T, MIXED, false, true><<<h->ntiles, ct, csmem, s>>>(p);
-    else if (cells) k_push_cells<T, MIXED, true, true><<<h->ntiles, ct, csmem, s>>>(p);
-    else if (!compat) k_push<T, MIXED, true, false, true><<<h->ntiles, nt, smem, s>>>(p);
+    if (!compat) k_push<T, MIXED, true, false, true><<<h->ntiles, nt, smem, s>>>(p);
     else k_push<T, MIXED, true, true, true><<<h->ntiles, nt, smem, s>>>(p);
     CKLAUNCH("k_push");
     h->cur = o;
     h->lazy = false;
   } else {
-    if (cells && hist && !compat) k_push_cells<T, MIXED, false, false><<<h->ntiles, ct, csmem, s>>>(p);
-    else if (cells && hist) k_push_cells<T, MIXED, true, false><<<h->ntiles, ct, csmem, s>>>(p);
-    else if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
+    if (hist && !compat) k_push<T, MIXED, true, false><<<h->ntiles, nt, smem, s>>>(p);
     else if (hist) k_push<T, MIXED, true, true><<<h->ntiles, nt, smem, s>>>(p);
     else if (!compat) k_push<T, MIXED, false, false><<<h->ntiles, nt, smem, s>>>(p);
     else k_push<T, MIXED, false, true><<<h->ntiles, nt, smem, s>>>(p);
@@ -578,7 +536,6 @@ int do_push(pbpic_handle* h) {
   k_energy_row<<<1, 256, 0, s>>>(h->ke_part, h->ntiles, nullptr, 0, 0, 0, h->hist + (size_t)(h->itime + 1) * 4);
   CKLAUNCH("k_energy_row");
   h->hist_valid = hist;
-  h->ranks_valid = p.rankw != nullptr;
   h->sorted = false;
   if (autosort) TRY((do_fused_sort<T, MIXED>(h)));
   return PBPIC_OK;
@@ -625,14 +582,8 @@ int do_fused_sort(pbpic_handle* h) {
   if (n > 0) {  // the sorted order as a permutation; the particle data stay in place
     if (!h->perm) TRY(dalloc(h, &h->perm, ((size_t)std::max<int64_t>(h->cap, 1) + 16) * 4));
     sp.perm = h->perm;
-    if (h->ranks_valid && h->TY <= 64) {
-      RankParams rp{h->TY, h->nb, h->tile_off, h->tbase, h->rankw, h->ctab, h->perm};
-      k_fused_perm_rw<<<h->ntiles, 256, 0, s>>>(rp);
-      CKLAUNCH("k_fused_perm_rw");
-    } else {
-      k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp);
-      CKLAUNCH("k_fused_perm");
-    }
+    k_fused_perm<T><<<h->ntiles, 256, 0, s>>>(sp);
+    CKLAUNCH("k_fused_perm");
     h->lazy = true;
   }
   k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, h->cfg.my,
@@ -640,7 +591,6 @@ int do_fused_sort(pbpic_handle* h) {
   CKLAUNCH("k_tile_off");
   h->sorted = true;
   h->hist_valid = false;
-  h->ranks_valid = false;
   return PBPIC_OK;
 }
 
@@ -959,8 +909,7 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
     return fail(PBPIC_EINVAL, "unknown precision");
   if (c.capacity < 0 || c.capacity > 0x7fffff00ll) return fail(PBPIC_EINVAL, "capacity must be in [0, 2^31)");
   if (c.compat & ~7) return fail(PBPIC_EINVAL, "unknown compat bits");
-  if (c.options & ~(PBPIC_OPT_NO_AUTOSORT | PBPIC_OPT_EXACT_FP64 | PBPIC_OPT_TILE_PUSH))
-    return fail(PBPIC_EINVAL, "unknown option bits");
+  if (c.options & ~(PBPIC_OPT_NO_AUTOSORT | PBPIC_OPT_EXACT_FP64)) return fail(PBPIC_EINVAL, "unknown option bits");
   const double cfl = c.cva * c.dt * sqrt(1.0 / (c.dx * c.dx) + 1.0 / (c.dy * c.dy));
   if (!(cfl < 1.0)) return fail(PBPIC_EINVAL, "time step violates the CFL condition c*dt*sqrt(1/dx^2+1/dy^2) < 1");
   if (c.cva * c.dt / std::min(c.dx, c.dy) >= 1.0)
@@ -2576,7 +2525,6 @@ int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_
   CKLAUNCH("k_tile_off");
   h->sorted = true;
   h->hist_valid = false;
-  h->ranks_valid = false;
   return PBPIC_OK;
 }
 

@@ -28,8 +28,7 @@ module pbpic_gpu
     integer(c_int32_t), parameter :: PBPIC_BC_PERIODIC = 0, PBPIC_BC_CONDUCTING = 1
     integer(c_int32_t), parameter :: PBPIC_FP64_PLAIN = 0, PBPIC_FP32_MIXED = 1
     integer(c_int32_t), parameter :: PBPIC_COMPAT_BORIS = 1, PBPIC_COMPAT_FOLD = 2, PBPIC_COMPAT_RHO = 4
-    integer(c_int32_t), parameter :: PBPIC_OPT_NO_AUTOSORT = 1, PBPIC_OPT_EXACT_FP64 = 2, &
-                                     PBPIC_OPT_TILE_PUSH = 4
+    integer(c_int32_t), parameter :: PBPIC_OPT_NO_AUTOSORT = 1, PBPIC_OPT_EXACT_FP64 = 2
     integer(c_int32_t), parameter :: PBPIC_FILTER_MARDER = 1, PBPIC_FILTER_CERENKOV = 2
     integer(c_int32_t), parameter :: PBPIC_LOAD_UNIFORM = 0, PBPIC_LOAD_HARRIS = 1, PBPIC_LOAD_TWO_STREAM = 2, &
                                      PBPIC_LOAD_WEIBEL = 3, PBPIC_LOAD_DOUBLE_HARRIS = 4

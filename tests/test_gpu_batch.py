@@ -1,9 +1,8 @@
 """The batched form against independent single-domain handles.
 
 A domain stepped in a batch runs the same arithmetic as pbpic_step(h, n, 1)
-on a handle with the same tile rows, 8 particles per thread and the tile push
-(PBPIC_OPT_TILE_PUSH), so with groups = 2 its particles, fields and energy
-history must be bit-identical.
+on a handle with the same tile rows and 8 particles per thread, so with
+groups = 2 its particles, fields and energy history must be bit-identical.
 Other tilings change only the FP32 summation order of the current; they are
 checked through charge conservation and the energy. With a charge-conserving
 deposit, div E / cva^2 - rho keeps its initial value at every node, so the
@@ -30,9 +29,8 @@ def small_domains():
 
 def single_run(cfg, ld, tile_rows, steps):
     from pbpic_b200.sim import Simulation
-    import pbpic_b200
     sim = Simulation.from_config(cfg, precision="fp32", tile_rows=int(tile_rows),
-                                 capacity=2 * ld["ppc"] * cfg["mx"] * cfg["my"], options=pbpic_b200.OPT_TILE_PUSH)
+                                 capacity=2 * ld["ppc"] * cfg["mx"] * cfg["my"])
     sim.init_plasma(**ld)
     sim.step(steps, sort_every=1)
     return sim
