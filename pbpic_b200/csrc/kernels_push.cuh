@@ -181,6 +181,17 @@ template <class T, bool MIXED, bool COMPAT = true>
 __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux, T puy,
                                           T puz, T ex, T ey, T ez, T bx, T by, T bz, Pushed<T>& o);
 
+// A species constant of the push (index 0 ion, 1 electron): an indexed read of
+// the parameter array (PBPIC_PUSH_IDXCONST = 1) or a select of its two entries.
+#ifndef PBPIC_PUSH_IDXCONST
+#define PBPIC_PUSH_IDXCONST 0
+#endif
+#if PBPIC_PUSH_IDXCONST
+#define PBD_SPECIES(arr, sp) (arr)[(sp)]
+#else
+#define PBD_SPECIES(arr, sp) ((sp) ? (arr)[1] : (arr)[0])
+#endif
+
 // Push of one particle whose gather nodes are n00 (ix,iy), n01 (ix,iy+1),
 // n10 (ix+1,iy), n11 (ix+1,iy+1). MIXED is only instantiated with T = float.
 // COMPAT = false compiles the step for a configuration without the compat
@@ -223,7 +234,7 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
   using A = M<T, MIXED>;
   const T half = T(0.5), one = T(1);
   // Boris rotation, pic2d.f90:969-996
-  const T c0 = sp ? a.c0[1] : a.c0[0], c1 = sp ? a.c1[1] : a.c1[0];
+  const T c0 = PBD_SPECIES(a.c0, sp), c1 = PBD_SPECIES(a.c1, sp);
   const T umx = A::mad(c1, ex, pux), umy = A::mad(c1, ey, puy), umz = A::mad(c1, ez, puz);
   const T g2m = A::mad(umz, umz, A::mad(umy, umy, A::mad(umx, umx, one)));
   T c2, t2;
@@ -279,7 +290,7 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
   int st = 0;
   if (A::abs(dx1) > T(1.5) || A::abs(dy1) > T(1.5)) st |= 1;
   if (!(gama < T(3.0e38))) st |= 2;  // NaN or overflow
-  const T msp = sp ? a.ms[1] : a.ms[0];
+  const T msp = PBD_SPECIES(a.ms, sp);
   if constexpr (MIXED) {  // (gamma - 1) = u^2 / (gamma + 1) avoids the cancellation of gamma - 1 in FP32
     const T usq = A::mad(uz, uz, A::mad(uy, uy, A::mul(ux, ux)));
     o.ke = A::mul(push_fdiv(usq, A::add(gama, one)), msp);
@@ -289,9 +300,9 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
 
   // ---- charge-conserving deposit terms (pic2d.f90:1237-1295), indices
   // relative to the old cell: i1 = j1 = 0, i2 = dcx, j2 = dcy.
-  const T qx = sp ? a.qx[1] : a.qx[0], qy = sp ? a.qy[1] : a.qy[0], qq = sp ? a.q[1] : a.q[0];
+  const T qx = PBD_SPECIES(a.qx, sp), qy = PBD_SPECIES(a.qy, sp), qq = PBD_SPECIES(a.q, sp);
   T im, jm;
-  if constexpr (MIXED) {
+  if constexpr (MIXED || !COMPAT) {  // cell-relative form (the plain form's exact order below)
     // Positions in cell units from the old cell's lower-left node: start
     // xs = dx0 + 1/2, end xe = dx1 + 1/2 (= dcx + dx2 + 1/2). The relay point
     // is the midpoint for a particle that stays, else the face it crosses.
@@ -792,24 +803,25 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
             }
             acc_key = key;
           }
-          if constexpr (MIXED) {
-            acc[0] = __fadd_rn(acc[0], __fmaf_rn(-o.ja, o.jw, o.ja));
-            acc[1] = __fmaf_rn(o.ja, o.jw, acc[1]);
-            acc[2] = __fadd_rn(acc[2], __fmaf_rn(-o.jb, o.jv, o.jb));
-            acc[3] = __fmaf_rn(o.jb, o.jv, acc[3]);
+          if constexpr (MIXED || !COMPAT) {  // FMA forms of the cell-relative terms
+            using F = M<T, true>;
+            acc[0] = F::add(acc[0], F::mad(-o.ja, o.jw, o.ja));
+            acc[1] = F::mad(o.ja, o.jw, acc[1]);
+            acc[2] = F::add(acc[2], F::mad(-o.jb, o.jv, o.jb));
+            acc[3] = F::mad(o.jb, o.jv, acc[3]);
             // jz: outer product of the x weights (x = -1, 0, 1) and y weights
-            const T qs = __fmul_rn(o.quz, o.zdx), q0 = __fsub_rn(o.quz, qs);
+            const T qs = F::mul(o.quz, o.zdx), q0 = F::sub(o.quz, qs);
             const T qxm = o.di < 0 ? qs : T(0), qxp = o.di > 0 ? qs : T(0);
-            const T ym = o.dj < 0 ? o.zdy : T(0), yp = o.dj > 0 ? o.zdy : T(0), y0 = __fsub_rn(T(1), o.zdy);
-            acc[4 + 0] = __fmaf_rn(qxm, ym, acc[4 + 0]);
-            acc[4 + 1] = __fmaf_rn(qxm, y0, acc[4 + 1]);
-            acc[4 + 2] = __fmaf_rn(qxm, yp, acc[4 + 2]);
-            acc[4 + 3] = __fmaf_rn(q0, ym, acc[4 + 3]);
-            acc[4 + 4] = __fmaf_rn(q0, y0, acc[4 + 4]);
-            acc[4 + 5] = __fmaf_rn(q0, yp, acc[4 + 5]);
-            acc[4 + 6] = __fmaf_rn(qxp, ym, acc[4 + 6]);
-            acc[4 + 7] = __fmaf_rn(qxp, y0, acc[4 + 7]);
-            acc[4 + 8] = __fmaf_rn(qxp, yp, acc[4 + 8]);
+            const T ym = o.dj < 0 ? o.zdy : T(0), yp = o.dj > 0 ? o.zdy : T(0), y0 = F::sub(T(1), o.zdy);
+            acc[4 + 0] = F::mad(qxm, ym, acc[4 + 0]);
+            acc[4 + 1] = F::mad(qxm, y0, acc[4 + 1]);
+            acc[4 + 2] = F::mad(qxm, yp, acc[4 + 2]);
+            acc[4 + 3] = F::mad(q0, ym, acc[4 + 3]);
+            acc[4 + 4] = F::mad(q0, y0, acc[4 + 4]);
+            acc[4 + 5] = F::mad(q0, yp, acc[4 + 5]);
+            acc[4 + 6] = F::mad(qxp, ym, acc[4 + 6]);
+            acc[4 + 7] = F::mad(qxp, y0, acc[4 + 7]);
+            acc[4 + 8] = F::mad(qxp, yp, acc[4 + 8]);
           } else {
             acc[0] += cross ? o.e[0] : o.e[0] + o.e[2];
             acc[1] += cross ? o.e[1] : o.e[1] + o.e[3];
