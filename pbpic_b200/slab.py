@@ -271,6 +271,8 @@ class SlabRun:
         inc = self.t.exchange(self.slabs, out)
         for r, e in self.slabs.items():
             lay = e.lay
+            if not (lay.has_down or lay.has_up):
+                continue  # a slab with no neighbours (one slab between walls) has no ghost rows
             from_down, from_up = inc[r]
             e.replace(lay.lo, lay.hi, from_down, lay.off_down, from_up, lay.off_up)
         # fields: own rows next to the neighbours into their ghost rows
