@@ -441,8 +441,10 @@ def gpu_slab_engine(cfg, ld, lay, precision="fp32"):
                                        ctypes.byref(cnt)))
         f = torch.empty(6 * cfg["mx"] * rows, dtype=ftype, device="cuda")
         L.check(lib.pbpic_field_rows_get(g.handle, lay.y0, rows, ctypes.c_void_p(f.data_ptr())))
-    # own particles, ghost bands of up to 8 rows (a sheet row holds up to 6x the mean) and slack
-    cap = own + 8 * 6 * (own // max(lay.own, 1)) + (1 << 20)
+    # own particles plus room for two sets of ghost bands (the bands a step receives are converted
+    # after the particles it holds, which include the last bands): 8 rows on each side, a sheet
+    # row holding up to 6x the mean
+    cap = own + 2 * 8 * 6 * (own // max(lay.own, 1)) + (1 << 20)
     e = GpuEngine(cfg, lay, precision, capacity=cap)
     e.append(band[: own * rec.itemsize], lay.row_offset)
     del band

@@ -308,4 +308,80 @@ __global__ void k_band_assemble(int64_t total, ReplaceSrc s, const RefRec<R>* bo
   }
 }
 
+// Band assembly without moving the slab's own particles: the received band
+// records are converted in place after the current particles (elements
+// base .. base + nb + nt of the current arrays: the bottom band, then the top
+// band), and the assembled cell order becomes a permutation -- each column's
+// bottom band, own rows, top band, as k_band_assemble writes them -- which the
+// next push reads through. The own particles stay where they are.
+template <class T, class R>
+__global__ void k_band_to_soa(int64_t nb, int64_t nt, ReplaceSrc s, const RefRec<R>* bot, const RefRec<R>* top,
+                              int64_t base, uint32_t* co, T* dxo, T* dyo, T* uxo, T* uyo, T* uzo, int32_t* pido,
+                              int* status) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nb + nt; k += (int64_t)gridDim.x * blockDim.x) {
+    const bool lower = k < nb;
+    const RefRec<R> rec = lower ? bot[k] : top[k - nb];
+    const int g = rec.grid - 1;
+    const int gx = g / s.my_global, gy = g - gx * s.my_global;
+    const int iy = gy - (lower ? s.off_bottom : s.off_top);
+    const bool ok = gx >= 0 && gx < s.mx && iy >= 0 && iy < s.my && (rec.q == 1 || rec.q == -1);
+    if (!ok) atomicOr(status, 8);
+    const int64_t e = base + k;
+    co[e] = ok ? cw_make(gx, iy, rec.q < 0 ? 1 : 0) : cw_make(gx >= 0 && gx < s.mx ? gx : 0, s.y_lo, 1);
+    dxo[e] = ok ? (T)rec.dx : T(0);
+    dyo[e] = ok ? (T)rec.dy : T(0);
+    uxo[e] = ok ? (T)rec.ux : T(0);
+    uyo[e] = ok ? (T)rec.uy : T(0);
+    uzo[e] = ok ? (T)rec.uz : T(0);
+    if (pido) pido[e] = rec.pid;
+  }
+}
+
+// Assembled position -> element of the current arrays, one block per column
+// (its positions outstart[ix] .. outstart[ix+1]: bottom band, own rows, top band).
+__global__ static void k_band_assemble_perm(ReplaceSrc s, int64_t base, int64_t nb_all, const int32_t* perm,
+                                            int32_t* out) {
+  for (int ix = blockIdx.x; ix < s.mx; ix += gridDim.x) {
+    const int64_t k0 = s.outstart[ix], k1 = s.outstart[ix + 1];
+    const int nb = s.bcnt[ix], no = s.ocnt[ix];
+    const int64_t own0 = s.off[(int64_t)ix * s.my + s.y_lo];
+    const int64_t b0 = base + s.bstart[ix], t0 = base + nb_all + s.tstart[ix];
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+      const int64_t r = k - k0;
+      int64_t e;
+      if (r < nb) {
+        e = b0 + r;
+      } else if (r < nb + no) {
+        const int64_t j = own0 + (r - nb);
+        e = perm ? (int64_t)perm[j] : j;
+      } else {
+        e = t0 + (r - nb - no);
+      }
+      out[k] = (int32_t)e;
+    }
+  }
+}
+
+// Cell counts of the assembled order: the own rows [y_lo, y_hi) keep their
+// counts (from the offsets before the assembly), the ghost rows count the
+// converted band records.
+__global__ static void k_counts_own_rows(const int32_t* off, int64_t ncells, int my, int y_lo, int y_hi,
+                                         int32_t* counts) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
+    if (c == ncells) {
+      counts[c] = 0;
+      continue;
+    }
+    const int row = (int)(c % my);
+    counts[c] = (row >= y_lo && row < y_hi) ? off[c + 1] - off[c] : 0;
+  }
+}
+
+__global__ static void k_counts_band(int64_t n, const uint32_t* cell, int64_t base, int my, int32_t* counts) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = cell[base + k];
+    atomicAdd(&counts[(int64_t)cw_ix(w) * my + cw_iy(w)], 1);
+  }
+}
+
 }  // namespace pbd

@@ -168,6 +168,7 @@ struct pbpic_handle {
   // through perm. The next push reads through it; every other reader of the
   // particle arrays applies it first (materialize).
   int32_t* perm = nullptr;
+  int32_t* perm2 = nullptr;  // the band assembly's permutation (swapped with perm)
   bool lazy = false;
   size_t push_optin = 0;    // dynamic shared memory the plain form's k_push may take
   int nb = 0;               // window bins per tile, 3*(TY+2)
@@ -2489,6 +2490,8 @@ int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_
   CK(cudaStreamSynchronize(s));
   if (total > h->cap) return fail(PBPIC_ECAPACITY, "the slab's particles and bands exceed the capacity");
   const int b = h->cur, o = 1 - b;
+  const int64_t base = h->n;  // the bands' records go after the current particles
+  const bool by_perm = base + nb + nt <= h->cap;
   ReplaceSrc rs;
   rs.off = h->off;
   rs.outstart = outstart;
@@ -2502,6 +2505,41 @@ int do_band_replace(pbpic_handle* h, int y_lo, int y_hi, const void* bot, int64_
   rs.off_bottom = off_bottom;
   rs.off_top = off_top;
   rs.tstart = tstart;
+  if (by_perm) {
+    // the own particles stay in place: the bands are converted after them and
+    // the assembled order is a permutation the next push reads through
+    if (nb + nt > 0) {
+      k_band_to_soa<T, T><<<grid_for(nb + nt, 256), 256, 0, s>>>(
+          nb, nt, rs, (const RefRec<T>*)bot, (const RefRec<T>*)top, base, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
+          P<T>(h, b, 2), P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], h->status);
+      CKLAUNCH("k_band_to_soa");
+    }
+    const int64_t pcap = std::max<int64_t>(h->cap, 1) + 16;
+    if (!h->perm) TRY(dalloc(h, &h->perm, (size_t)pcap * 4));
+    if (!h->perm2) TRY(dalloc(h, &h->perm2, (size_t)pcap * 4));
+    if (total > 0) {
+      k_band_assemble_perm<<<std::min(mx, 148 * 16), 256, 0, s>>>(rs, base, nb, h->lazy ? h->perm : nullptr, h->perm2);
+      CKLAUNCH("k_band_assemble_perm");
+    }
+    k_counts_own_rows<<<grid_for((int64_t)h->ncells + 1, 256), 256, 0, s>>>(h->off, h->ncells, my, y_lo, y_hi,
+                                                                            h->counts);
+    CKLAUNCH("k_counts_own_rows");
+    if (nb + nt > 0) {
+      k_counts_band<<<grid_for(nb + nt, 256), 256, 0, s>>>(nb + nt, h->cell[b], base, my, h->counts);
+      CKLAUNCH("k_counts_band");
+    }
+    std::swap(h->perm, h->perm2);
+    h->lazy = true;  // cell order = the current arrays read through perm
+    h->n = total;
+    CK(cudaMemcpyAsync(h->off, h->counts, (size_t)(h->ncells + 1) * 4, cudaMemcpyDeviceToDevice, s));
+    TRY(scan_excl(s, h->off, h->ncells + 1, h->scan_scratch));
+    k_tile_off<<<grid_for(h->ntiles + 1, 256, 1 << 20), 256, 0, s>>>(h->off, h->ntiles, h->tpc, h->TY, my, total,
+                                                                    h->tile_off);
+    CKLAUNCH("k_tile_off");
+    h->sorted = true;
+    h->hist_valid = false;
+    return PBPIC_OK;
+  }
   if (total > 0) {
     k_band_assemble<T, T><<<grid_for(total, 256), 256, 0, s>>>(
         total, rs, (const RefRec<T>*)bot, (const RefRec<T>*)top, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1),
