@@ -760,6 +760,9 @@ def main():
     achieved_push = bytes_push / (m["t_push"] * 1e-3) / 1e9
     cells = cfg["mx"] * cfg["my"]
     step_bytes = 48.0 * n + (48.0 * n if args.sort_every == 1 else 48.0 * n / max(args.sort_every, 1)) + 60.0 * cells
+    # the bytes the step moves: the push's 48 B, the ranking's cell word read and permutation entry
+    # written (8 B) at each sort, the grid's 60 B per cell
+    step_moved = 48.0 * n + 8.0 * n / max(args.sort_every, 1) + 60.0 * cells
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -773,7 +776,8 @@ def main():
                      "kernel": PUSH_KERNEL,
                      "bytes_per_launch": bytes_push, "peak_kind": peak_kind,
                      "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": achieved_push / NOMINAL_HBM_GBS,
-                     "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak},
+                     "step_frac": step_bytes / (m["ms_per_step"] * 1e-3) / 1e9 / peak,
+                     "step_frac_moved": step_moved / (m["ms_per_step"] * 1e-3) / 1e9 / peak},
         "phase_ms": {"push": m["t_push"], "fieldsolve": m["t_field"], "sort": m["t_sort"]},
         "energy": {"mixed_drift": m["energy_drift"], "gauss_residual": m["gauss"], "reconnected_flux": m["flux"]},
         "gpu_launches": m["launches"],

@@ -604,54 +604,190 @@ __host__ __device__ __forceinline__ size_t push_first_offset(int ty) {
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
-// Push of tile t of the domain `a`, by all threads of the block. G float4
+// Shared-memory window of a tile push (smem_raw): the window (16*(ty+3)
+// accumulators), the new-cell histogram (3*(ty+2) int), then the mixed form's
+// crossers' windows (2 x 8*(ty+3) 32-bit sums) or the plain form's second stage.
+template <class T, bool MIXED>
+struct TileWin {
+  using Acc = typename std::conditional<MIXED, long long, double>::type;
+  int TY, WR, NB, ixt, y0, y1;
+  Acc* win;
+  int* hist;
+  unsigned* clo;  // crossers: jx, jy planes (8 * WR)
+  int* chi;
+};
+
+// Clears the windows of tile t and starts its histogram from the input's cell
+// counts: the input is sorted by cell, so every particle of a tile cell stays
+// in that cell's bin unless it crosses, and each crossing particle moves one
+// count.
+template <class T, bool MIXED, bool HIST>
+__device__ __forceinline__ TileWin<T, MIXED> tile_begin(const PushParams<T>& a, int t, unsigned char* smem_raw) {
+  using Acc = typename TileWin<T, MIXED>::Acc;
+  TileWin<T, MIXED> w;
+  w.TY = a.tile_rows;
+  w.WR = w.TY + 3;
+  w.NB = 3 * (w.TY + 2);
+  w.win = reinterpret_cast<Acc*>(smem_raw);
+  w.hist = reinterpret_cast<int*>(w.win + 16 * w.WR);
+  w.clo = reinterpret_cast<unsigned*>(w.hist + w.NB);
+  w.chi = reinterpret_cast<int*>(w.clo + 8 * w.WR);
+  w.ixt = t / a.tiles_per_col;
+  w.y0 = (t - w.ixt * a.tiles_per_col) * w.TY;
+  w.y1 = min(w.y0 + w.TY, a.my);
+  for (int e = threadIdx.x; e < 16 * w.WR; e += blockDim.x) w.win[e] = Acc(0);
+  if (MIXED)
+    for (int e = threadIdx.x; e < 8 * w.WR; e += blockDim.x) {
+      w.clo[e] = 0u;
+      w.chi[e] = 0;
+    }
+  if (HIST)
+    for (int e = threadIdx.x; e < w.NB; e += blockDim.x) {
+      const int by = e - (w.TY + 2);
+      int v = 0;
+      if (by >= 1 && by <= w.y1 - w.y0) {
+        const long long c = (long long)w.ixt * a.my + w.y0 + by - 1;
+        v = a.cell_off[c + 1] - a.cell_off[c];
+      }
+      w.hist[e] = v;
+    }
+  __syncthreads();
+  return w;
+}
+
+// A crossing particle (old cell (ix, iy) in tile window w) moves one count of
+// the histogram from its old cell's bin to its new cell's. Returns the status
+// bits it raises (a jump of two cells, only from a corrupt offset, keeps the
+// particle in its cell: *cw is reset to the old word).
+template <class T, bool MIXED>
+__device__ __forceinline__ int hist_move(const PushParams<T>& a, const TileWin<T, MIXED>& w, uint32_t old_cw,
+                                         uint32_t* cw, int dcx, int ix, int iy) {
+  int st = 0;
+  // new cell in the tile's window: column 1 + dcx, row new_iy - y0 + 1
+  // (wrapped rows come back through +-my; a reflected particle keeps its row)
+  int by = cw_iy(*cw) - w.y0 + 1;
+  by = by < 0 ? by + a.my : (by > w.y1 - w.y0 + 1 ? by - a.my : by);
+  int b = (1 + dcx) * (w.TY + 2) + by;
+  if (by < 0 || by > w.y1 - w.y0 + 1) {
+    b = window_bin(cw_ix(*cw), cw_iy(*cw), w.ixt, w.y0, w.y1, w.TY, a.mx, a.my, a.ybc);
+    if (b < 0) {
+      st = 1;
+      *cw = old_cw;
+      b = window_bin(ix, iy, w.ixt, w.y0, w.y1, w.TY, a.mx, a.my, a.ybc);
+    }
+  }
+  const int bo = (w.TY + 2) + iy - w.y0 + 1;  // the old cell's bin
+  if (b != bo) {
+    atomicAdd(&w.hist[b], 1);
+    atomicAdd(&w.hist[bo], -1);
+  }
+  return st;
+}
+
+// End of a pass: sum the stencils of lanes that share a cell; 17 lanes add
+// each run's sum to the window. stage: the warp's [17][33] staging rows;
+// fw: the warp's [17][33] first parts; vals(k): this lane's stencil entry k.
+template <class T, bool MIXED, class Vals>
+__device__ __forceinline__ void pass_sums(const Vals& vals, int acc_key, int first_key, T (*stage)[33], const T* fw,
+                                          typename std::conditional<MIXED, long long, double>::type* win, int WR,
+                                          int sc, int sx, int sy) {
+  const unsigned lane = lane_id();
+  T* mycol = &stage[0][lane];
+  const int key = acc_key >= 0 ? acc_key : -1 - (int)lane;
+  const int kprev = __shfl_up_sync(FULL, key, 1);
+  const unsigned head = (lane == 0) || (kprev != key);
+  // Keys do not decrease across the lanes, so a run is the lanes head..tail
+  // plus, when the next lane's first part has the run's cell, that part. The
+  // 17 lanes sum the run's staged columns in lane order (a fixed order: the
+  // result does not depend on timing). A first part that does not continue
+  // the run ending at the previous lane is added on its own.
+  const int fnext = __shfl_down_sync(FULL, first_key, 1);
+  const unsigned heads = __ballot_sync(FULL, head);
+  const unsigned head_next = __shfl_down_sync(FULL, head, 1);
+  unsigned tails = __ballot_sync(FULL, acc_key >= 0 && (lane == 31 || head_next));
+  const bool joined = lane > 0 && head && kprev == first_key;
+  unsigned solo = __ballot_sync(FULL, first_key >= 0 && !joined);
+#pragma unroll
+  for (int k = 0; k < 17; ++k) mycol[k * 33] = vals(k);
+  __syncwarp();
+  while (tails) {
+    const int src = __ffs(tails) - 1;
+    tails &= tails - 1;
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - src)));
+    const int kt = __shfl_sync(FULL, key, src);
+    const int nf = __shfl_sync(FULL, fnext, src);
+    if (lane < 17) {
+      const T* row = &stage[lane][0];
+      T v = row[start];
+      for (int l = start + 1; l <= src; ++l) v = add_rn(v, row[l]);
+      if (src < 31 && nf == kt) v = add_rn(v, fw[lane * 33 + src + 1]);
+      if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+    }
+  }
+  while (solo) {
+    const int src = __ffs(solo) - 1;
+    solo &= solo - 1;
+    const int kt = __shfl_sync(FULL, first_key, src);
+    if (lane < 17) {
+      const T v = fw[lane * 33 + src];
+      if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
+    }
+  }
+  __syncwarp();  // the stage is rewritten in the next pass
+}
+
+// End of a tile: fold the window into the global current, write the tile's
+// histogram, kinetic energies and status.
+template <class T, bool MIXED, bool HIST>
+__device__ __forceinline__ void tile_end(const PushParams<T>& a, int t, const TileWin<T, MIXED>& w, double ke_e,
+                                         double ke_i, int status, double* red) {
+  using Acc = typename TileWin<T, MIXED>::Acc;
+  Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
+  __syncthreads();
+  for (int e = threadIdx.x; e < 16 * w.WR; e += blockDim.x) {
+    Acc val = w.win[e];
+    if (MIXED && e < 8 * w.WR) val += (Acc)(((long long)w.chi[e] << 17) + (long long)w.clo[e]);
+    if (val == Acc(0)) continue;
+    const int c = e / (4 * w.WR);
+    const int r = e - c * 4 * w.WR;
+    const int wx = r / w.WR, wy = r - wx * w.WR;
+    long long gi;
+    int sg;
+    if (map_current(c, w.ixt - 1 + wx, w.y0 - 1 + wy, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
+      acc_add(&gacc[gi], sg < 0 ? -val : val);
+  }
+  if (HIST)
+    for (int e = threadIdx.x; e < w.NB; e += blockDim.x) a.tilecnt[(long long)t * w.NB + e] = w.hist[e];
+  const double se = block_sum(ke_e, red);
+  const double si = block_sum(ke_i, red);
+  if (threadIdx.x == 0) {
+    a.ke_part[2 * t] = se;
+    a.ke_part[2 * t + 1] = si;
+  }
+  status = __reduce_or_sync(FULL, status);
+  if (lane_id() == 0 && status) atomicOr(a.status, status);
+}
+
+// Push of tile t of the domain `a`, by all threads of the block: G float4
 // groups of particles per thread per pass (8 particles for G = 2).
-// smem_raw: window (16*(ty+3) accumulators), histogram (3*(ty+2) int), then the
-// mixed form's crossers' windows or the plain form's second stage.
 template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true, bool GATHER = false>
 __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
                                           unsigned char* smem_raw) {
-  using Acc = typename std::conditional<MIXED, long long, double>::type;
   constexpr int PT = 4 * G;  // particles per thread per pass
-  const int TY = a.tile_rows, WR = TY + 3, NB = 3 * (TY + 2);
-  Acc* win = reinterpret_cast<Acc*>(smem_raw);
-  int* hist = reinterpret_cast<int*>(win + 16 * WR);
-  unsigned* clo = reinterpret_cast<unsigned*>(hist + NB);  // crossers: jx, jy planes (8 * WR)
-  int* chi = reinterpret_cast<int*>(clo + 8 * WR);
-  // [warp][17][33] first parts of the lanes whose particles change cell (the
-  // mixed form's static array keeps its addresses constant)
-  auto first = [&](int w_, int k_, int l_) -> T& {
-    if constexpr (MIXED) return sm.first[w_][k_][l_];
-    else return reinterpret_cast<T*>(smem_raw + push_first_offset(TY))[(w_ * 17 + k_) * 33 + l_];
-  };
-  const int ixt = t / a.tiles_per_col;
-  const int y0 = (t - ixt * a.tiles_per_col) * TY;
-  const int y1 = min(y0 + TY, a.my);
-  for (int e = threadIdx.x; e < 16 * WR; e += blockDim.x) win[e] = Acc(0);
-  if (MIXED)
-    for (int e = threadIdx.x; e < 8 * WR; e += blockDim.x) {
-      clo[e] = 0u;
-      chi[e] = 0;
-    }
-  // The input is sorted by cell, so every particle of a tile cell stays in
-  // that cell's bin unless it crosses: the counts start from the input's cell
-  // counts and each crossing particle moves one count.
-  if (HIST)
-    for (int e = threadIdx.x; e < NB; e += blockDim.x) {
-      const int by = e - (TY + 2);
-      int v = 0;
-      if (by >= 1 && by <= y1 - y0) {
-        const long long c = (long long)ixt * a.my + y0 + by - 1;
-        v = a.cell_off[c + 1] - a.cell_off[c];
-      }
-      hist[e] = v;
-    }
-  __syncthreads();
-  Acc* gacc = reinterpret_cast<Acc*>(a.jacc);
+  const TileWin<T, MIXED> tw = tile_begin<T, MIXED, HIST>(a, t, smem_raw);
+  const int TY = tw.TY, WR = tw.WR, ixt = tw.ixt, y0 = tw.y0, y1 = tw.y1;
+  auto* win = tw.win;
+  unsigned* clo = tw.clo;
+  int* chi = tw.chi;
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
   const bool split = MIXED && pend - pbeg <= 32767;  // crossers to the 32-bit windows
   const unsigned lane = lane_id();
   const int w = threadIdx.x >> 5;
+  // [17][33] first parts of the lanes of warp w whose particles change cell
+  // (the mixed form's static array keeps its addresses constant)
+  T* fw;
+  if constexpr (MIXED) fw = &sm.first[w][0][0];
+  else fw = reinterpret_cast<T*>(smem_raw + push_first_offset(TY)) + w * 17 * 33;
   // this lane's entry of the stencil when it deposits a run's sum
   int sc = 0, sx = 0, sy = 0;
   stencil_node(lane < 17 ? (int)lane : 0, &sc, &sx, &sy);
@@ -664,7 +800,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 #pragma unroll
     for (int k = 0; k < 17; ++k) acc[k] = T(0);
     int acc_key = -1;
-    int first_key = -1;  // cell of this pass's finished first part (in `first`), or -1
+    int first_key = -1;  // cell of this pass's finished first part (in `fw`), or -1
     int cache_cell = -1;
     Node6<T> n00{}, n01{}, n10{}, n11{};
     CellCoef cc;  // mixed form with coefficient records
@@ -760,26 +896,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         status |= o.status;
         const bool inwin = ix == ixt && iy >= y0 && iy < y1;
         const bool cross = o.dcx != 0 || o.dcy != 0;
-        if (HIST && cross && inwin) {
-          // new cell in the tile's window: column 1 + dcx, row new_iy - y0 + 1
-          // (wrapped rows come back through +-my; a reflected particle keeps its row)
-          int by = cw_iy(o.cw) - y0 + 1;
-          by = by < 0 ? by + a.my : (by > y1 - y0 + 1 ? by - a.my : by);
-          int b = (1 + o.dcx) * (TY + 2) + by;
-          if (!inwin || by < 0 || by > y1 - y0 + 1) {
-            b = window_bin(cw_ix(o.cw), cw_iy(o.cw), ixt, y0, y1, TY, a.mx, a.my, a.ybc);
-            if (b < 0) {  // only a corrupt offset can jump two cells: keep the particle in its cell
-              status |= 1;
-              o.cw = wrd;
-              b = window_bin(ix, iy, ixt, y0, y1, TY, a.mx, a.my, a.ybc);
-            }
-          }
-          const int bo = (TY + 2) + iy - y0 + 1;  // the old cell's bin
-          if (b != bo) {
-            atomicAdd(&hist[b], 1);
-            atomicAdd(&hist[bo], -1);
-          }
-        }
+        if (HIST && cross && inwin) status |= hist_move<T, MIXED>(a, tw, wrd, &o.cw, o.dcx, ix, iy);
         if (inwin) {
           const int key = iy - y0;
           if (key != acc_key) {
@@ -788,7 +905,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
                 first_key = acc_key;
 #pragma unroll
                 for (int k = 0; k < 17; ++k) {
-                  first(w, k, lane) = acc[k];
+                  fw[k * 33 + lane] = acc[k];
                   acc[k] = T(0);
                 }
               }
@@ -908,73 +1025,9 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     }
     ke_e += (double)pke_e;
     ke_i += (double)pke_i;
-    // Sum the stencils of lanes that share a cell; 17 lanes add each run's sum.
-    const int key = acc_key >= 0 ? acc_key : -1 - (int)lane;
-    const int kprev = __shfl_up_sync(FULL, key, 1);
-    const unsigned head = (lane == 0) || (kprev != key);
-    // Keys do not decrease across the lanes, so a run is the lanes head..tail
-    // plus, when the next lane's first part has the run's cell, that part. The
-    // 17 lanes sum the run's staged columns in lane order (a fixed order: the
-    // result does not depend on timing). A first part that does not continue
-    // the run ending at the previous lane is added on its own.
-    const int fnext = __shfl_down_sync(FULL, first_key, 1);
-    const unsigned heads = __ballot_sync(FULL, head);
-    const unsigned head_next = __shfl_down_sync(FULL, head, 1);
-    unsigned tails = __ballot_sync(FULL, acc_key >= 0 && (lane == 31 || head_next));
-    const bool joined = lane > 0 && head && kprev == first_key;
-    unsigned solo = __ballot_sync(FULL, first_key >= 0 && !joined);
-#pragma unroll
-    for (int k = 0; k < 17; ++k) mycol[k * 33] = acc[k];
-    __syncwarp();
-    while (tails) {
-      const int src = __ffs(tails) - 1;
-      tails &= tails - 1;
-      const int start = 31 - __clz(heads & (0xffffffffu >> (31 - src)));
-      const int kt = __shfl_sync(FULL, key, src);
-      const int nf = __shfl_sync(FULL, fnext, src);
-      if (lane < 17) {
-        const T* row = &sm.stage[w][lane][0];
-        T v = row[start];
-        for (int l = start + 1; l <= src; ++l) v = add_rn(v, row[l]);
-        if (src < 31 && nf == kt) v = add_rn(v, first(w, lane, src + 1));
-        if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
-      }
-    }
-    while (solo) {
-      const int src = __ffs(solo) - 1;
-      solo &= solo - 1;
-      const int kt = __shfl_sync(FULL, first_key, src);
-      if (lane < 17) {
-        const T v = first(w, lane, src);
-        if (v != T(0)) acc_add(&win[(sc * 4 + 1 + sx) * WR + kt + 1 + sy], to_acc<T, MIXED>(v));
-      }
-    }
-    __syncwarp();  // the stage is rewritten in the next pass
+    pass_sums<T, MIXED>([&](int k) { return acc[k]; }, acc_key, first_key, sm.stage[w], fw, win, WR, sc, sx, sy);
   }
-  __syncthreads();
-  // Fold the window into the global current.
-  for (int e = threadIdx.x; e < 16 * WR; e += blockDim.x) {
-    Acc val = win[e];
-    if (MIXED && e < 8 * WR) val += (Acc)(((long long)chi[e] << 17) + (long long)clo[e]);
-    if (val == Acc(0)) continue;
-    const int c = e / (4 * WR);
-    const int r = e - c * 4 * WR;
-    const int wx = r / WR, wy = r - wx * WR;
-    long long gi;
-    int sg;
-    if (map_current(c, ixt - 1 + wx, y0 - 1 + wy, a.mx, a.my, a.S, a.ybc, a.compat, &gi, &sg))
-      acc_add(&gacc[gi], sg < 0 ? -val : val);
-  }
-  if (HIST)
-    for (int e = threadIdx.x; e < NB; e += blockDim.x) a.tilecnt[(long long)t * NB + e] = hist[e];
-  const double se = block_sum(ke_e, sm.red);
-  const double si = block_sum(ke_i, sm.red);
-  if (threadIdx.x == 0) {
-    a.ke_part[2 * t] = se;
-    a.ke_part[2 * t + 1] = si;
-  }
-  status = __reduce_or_sync(FULL, status);
-  if (lane == 0 && status) atomicOr(a.status, status);
+  tile_end<T, MIXED, HIST>(a, t, tw, ke_e, ke_i, status, sm.red);
 }
 
 // Single domain: one block per tile. COMPAT = false when no compat switch is
