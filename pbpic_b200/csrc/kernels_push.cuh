@@ -196,13 +196,15 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
 // n10 (ix+1,iy), n11 (ix+1,iy+1). MIXED is only instantiated with T = float.
 // COMPAT = false compiles the step for a configuration without the compat
 // switches of the push (the rho weights are then the gather weights) and, in
-// the plain form, forms 1/gamma with rsqrt; COMPAT = true keeps the
-// reference's correctly rounded quotients and square roots, bit for bit.
+// the plain form, forms 1/gamma with rsqrt and contracts a*b+c into one
+// fused multiply-add; COMPAT = true keeps the reference's correctly rounded
+// quotients and square roots and its separately rounded products and sums,
+// bit for bit.
 template <class T, bool MIXED, bool COMPAT = true>
 __device__ __forceinline__ void push_one(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux,
                                          T puy, T puz, const Node6<T>& n00, const Node6<T>& n01,
                                          const Node6<T>& n10, const Node6<T>& n11, Pushed<T>& o) {
-  using A = M<T, MIXED>;
+  using A = M<T, MIXED || !COMPAT>;  // fused multiply-adds except in the exact order
   const T half = T(0.5), one = T(1);
   // CIC weights, pic2d.f90:948-951
   const T axw = A::add(half, px), ayw = A::add(half, py);
@@ -231,7 +233,7 @@ __device__ __forceinline__ void push_one_coef(const PushParams<float>& a, int sp
 template <class T, bool MIXED, bool COMPAT>
 __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix, int iy, T px, T py, T pux, T puy,
                                           T puz, T ex, T ey, T ez, T bx, T by, T bz, Pushed<T>& o) {
-  using A = M<T, MIXED>;
+  using A = M<T, MIXED || !COMPAT>;  // fused multiply-adds except in the exact order
   const T half = T(0.5), one = T(1);
   // Boris rotation, pic2d.f90:969-996
   const T c0 = PBD_SPECIES(a.c0, sp), c1 = PBD_SPECIES(a.c1, sp);
