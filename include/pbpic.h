@@ -323,7 +323,8 @@ int pbpic_band_replace(pbpic_handle* h, int32_t y_lo, int32_t y_hi, const void* 
                        int32_t off_bottom, const void* top_dev, int64_t nt, int32_t off_top, int32_t my_global);
 /* Rows j0 .. j0+nrows-1 of the six field planes to / from device memory as
  * [6][mx][nrows] values of the handle's precision; setting them recomputes
- * the node averages. */
+ * the node averages and the push's gather records that those rows feed (the
+ * energy history is not rewritten). */
 int pbpic_field_rows_get(pbpic_handle* h, int32_t j0, int32_t nrows, void* dst_dev);
 int pbpic_field_rows_set(pbpic_handle* h, int32_t j0, int32_t nrows, const void* src_dev);
 /* Energies (electron KE, ion KE, E, B) of the particles in rows [y_lo,

@@ -140,43 +140,50 @@ __global__ void k_efull(FieldParams<T> a) {
 // Block `bid` of `nblk` writes partial sums `bid` (the partition of the sums,
 // and so their rounding, depends only on nblk).
 template <class T>
+__device__ __forceinline__ void node_at(const FieldParams<T>& a, int ia, int b, T& e2, T& b2) {
+  const int NY = a.my + 1;
+  const int i = ia == a.mx ? 0 : ia;
+  const int im = wrapx(i - 1, a.mx);
+  const long long oi = (long long)i * a.S, om = (long long)im * a.S;
+  const int bn = (a.ybc == 0 && b == a.my) ? 0 : b;  // node row
+  const T ex = (a.ex[oi + bn] + a.ex[om + bn]) * T(0.5);
+  const T bx = (a.bx[oi + bn] + a.bx[om + bn]) * T(0.5);
+  const T ey = (half_row(a.ey, i, b, a.my, a.S, a.ybc, T(1)) +
+                half_row(a.ey, i, b - 1, a.my, a.S, a.ybc, T(1))) * T(0.5);
+  const T by = (half_row(a.by, i, b, a.my, a.S, a.ybc, T(-1)) +
+                half_row(a.by, i, b - 1, a.my, a.S, a.ybc, T(-1))) * T(0.5);
+  const T ez = (half_row(a.ez, i, b, a.my, a.S, a.ybc, T(-1)) +
+                half_row(a.ez, im, b, a.my, a.S, a.ybc, T(-1)) +
+                half_row(a.ez, i, b - 1, a.my, a.S, a.ybc, T(-1)) +
+                half_row(a.ez, im, b - 1, a.my, a.S, a.ybc, T(-1))) * T(0.25);
+  const T bz = (half_row(a.bz, i, b, a.my, a.S, a.ybc, T(1)) +
+                half_row(a.bz, im, b, a.my, a.S, a.ybc, T(1)) +
+                half_row(a.bz, i, b - 1, a.my, a.S, a.ybc, T(1)) +
+                half_row(a.bz, im, b - 1, a.my, a.S, a.ybc, T(1))) * T(0.25);
+  T* g = a.ng + ((long long)ia * NY + b) * 8;
+  g[0] = ex;
+  g[1] = ey;
+  g[2] = ez;
+  g[3] = T(0);
+  g[4] = bx;
+  g[5] = by;
+  g[6] = bz;
+  g[7] = T(0);
+  e2 = ex * ex + ey * ey + ez * ez;
+  b2 = bx * bx + by * by + bz * bz;
+}
+
+template <class T>
 __device__ __forceinline__ void nodes_body(const FieldParams<T>& a, double* red, int bid, int nblk) {
   const int NX = a.mx + 1, NY = a.my + 1;
   const long long n = (long long)NX * NY;
   double se = 0.0, sb = 0.0;
   for (long long k = bid * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)nblk * blockDim.x) {
     const int ia = (int)(k / NY), b = (int)(k - (long long)ia * NY);
-    const int i = ia == a.mx ? 0 : ia;
-    const int im = wrapx(i - 1, a.mx);
-    const long long oi = (long long)i * a.S, om = (long long)im * a.S;
-    const int bn = (a.ybc == 0 && b == a.my) ? 0 : b;  // node row
-    const T ex = (a.ex[oi + bn] + a.ex[om + bn]) * T(0.5);
-    const T bx = (a.bx[oi + bn] + a.bx[om + bn]) * T(0.5);
-    const T ey = (half_row(a.ey, i, b, a.my, a.S, a.ybc, T(1)) +
-                  half_row(a.ey, i, b - 1, a.my, a.S, a.ybc, T(1))) * T(0.5);
-    const T by = (half_row(a.by, i, b, a.my, a.S, a.ybc, T(-1)) +
-                  half_row(a.by, i, b - 1, a.my, a.S, a.ybc, T(-1))) * T(0.5);
-    const T ez = (half_row(a.ez, i, b, a.my, a.S, a.ybc, T(-1)) +
-                  half_row(a.ez, im, b, a.my, a.S, a.ybc, T(-1)) +
-                  half_row(a.ez, i, b - 1, a.my, a.S, a.ybc, T(-1)) +
-                  half_row(a.ez, im, b - 1, a.my, a.S, a.ybc, T(-1))) * T(0.25);
-    const T bz = (half_row(a.bz, i, b, a.my, a.S, a.ybc, T(1)) +
-                  half_row(a.bz, im, b, a.my, a.S, a.ybc, T(1)) +
-                  half_row(a.bz, i, b - 1, a.my, a.S, a.ybc, T(1)) +
-                  half_row(a.bz, im, b - 1, a.my, a.S, a.ybc, T(1))) * T(0.25);
-    T* g = a.ng + k * 8;
-    g[0] = ex;
-    g[1] = ey;
-    g[2] = ez;
-    g[3] = T(0);
-    g[4] = bx;
-    g[5] = by;
-    g[6] = bz;
-    g[7] = T(0);
+    T e2, b2;
+    node_at(a, ia, b, e2, b2);
     if (ia < a.mx && (a.ybc == 1 || b < a.my)) {
       const double w = (a.ybc == 1 && (b == 0 || b == a.my)) ? 0.5 : 1.0;
-      const T e2 = ex * ex + ey * ey + ez * ez;
-      const T b2 = bx * bx + by * by + bz * bz;
       se += w * (double)e2;
       sb += w * (double)b2;
     }
@@ -186,6 +193,19 @@ __device__ __forceinline__ void nodes_body(const FieldParams<T>& a, double* red,
   if (threadIdx.x == 0) {
     a.fe_part[2 * bid] = te;
     a.fe_part[2 * bid + 1] = tb;
+  }
+}
+
+// Node averages of node rows [b0, b1) only (after a few field rows were set),
+// the same values as the whole-grid pass; no energy sums.
+template <class T>
+__global__ void k_nodes_rows(FieldParams<T> a, int b0, int b1) {
+  const int R = b1 - b0;
+  const long long n = (long long)(a.mx + 1) * R;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int ia = (int)(k / R), b = b0 + (int)(k - (long long)ia * R);
+    T e2, b2;
+    node_at(a, ia, b, e2, b2);
   }
 }
 
@@ -200,37 +220,52 @@ __global__ void k_nodes(FieldParams<T> a) {
 // bilinear coefficients (A, B, C, D) of each of ex ey ez bx by bz over the cell
 // (with PBPIC_CELL_COEF = 0 the 4 nodes themselves), as 6 contiguous 16-byte
 // stores, so the push reads a cell's gather data with 6 loads from one address.
+__device__ __forceinline__ void cell_record(const FieldParams<float>& a, int cx, int cy) {
+  const long long c = (long long)cx * a.my + cy;
+  const float4* g00 = reinterpret_cast<const float4*>(a.ng + ((long long)cx * (a.my + 1) + cy) * 8);
+  const float4* g10 = g00 + 2 * (long long)(a.my + 1);
+  const float4 p0 = g00[0], q0 = g00[1], p1 = g00[2], q1 = g00[3];  // nodes 00, 01: ex ey ez 0 | bx by bz 0
+  const float4 p2 = g10[0], q2 = g10[1], p3 = g10[2], q3 = g10[3];  // nodes 10, 11
+  float4* r = reinterpret_cast<float4*>(a.cg + c * 24);
+#if PBPIC_CELL_COEF
+  // per field: A = mean of the 4 nodes, B = x slope, C = y slope, D = twist
+  auto coef = [](float n00, float n01, float n10, float n11) {
+    const float sx0 = __fadd_rn(n00, n01), sx1 = __fadd_rn(n10, n11);
+    const float sy0 = __fadd_rn(n00, n10), sy1 = __fadd_rn(n01, n11);
+    return make_float4(__fmul_rn(0.25f, __fadd_rn(sx0, sx1)), __fmul_rn(0.5f, __fsub_rn(sx1, sx0)),
+                       __fmul_rn(0.5f, __fsub_rn(sy1, sy0)), __fsub_rn(__fsub_rn(n11, n10), __fsub_rn(n01, n00)));
+  };
+  r[0] = coef(p0.x, p1.x, p2.x, p3.x);
+  r[1] = coef(p0.y, p1.y, p2.y, p3.y);
+  r[2] = coef(p0.z, p1.z, p2.z, p3.z);
+  r[3] = coef(q0.x, q1.x, q2.x, q3.x);
+  r[4] = coef(q0.y, q1.y, q2.y, q3.y);
+  r[5] = coef(q0.z, q1.z, q2.z, q3.z);
+#else
+  r[0] = make_float4(p0.x, p0.y, p0.z, q0.x);
+  r[1] = make_float4(q0.y, q0.z, p1.x, p1.y);
+  r[2] = make_float4(p1.z, q1.x, q1.y, q1.z);
+  r[3] = make_float4(p2.x, p2.y, p2.z, q2.x);
+  r[4] = make_float4(q2.y, q2.z, p3.x, p3.y);
+  r[5] = make_float4(p3.z, q3.x, q3.y, q3.z);
+#endif
+}
+
 __device__ __forceinline__ void cell_records_body(const FieldParams<float>& a, int bid, int nblk) {
   const long long n = (long long)a.mx * a.my;
   for (long long c = bid * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)nblk * blockDim.x) {
     const int cx = (int)(c / a.my), cy = (int)(c - (long long)cx * a.my);
-    const float4* g00 = reinterpret_cast<const float4*>(a.ng + ((long long)cx * (a.my + 1) + cy) * 8);
-    const float4* g10 = g00 + 2 * (long long)(a.my + 1);
-    const float4 p0 = g00[0], q0 = g00[1], p1 = g00[2], q1 = g00[3];  // nodes 00, 01: ex ey ez 0 | bx by bz 0
-    const float4 p2 = g10[0], q2 = g10[1], p3 = g10[2], q3 = g10[3];  // nodes 10, 11
-    float4* r = reinterpret_cast<float4*>(a.cg + c * 24);
-#if PBPIC_CELL_COEF
-    // per field: A = mean of the 4 nodes, B = x slope, C = y slope, D = twist
-    auto coef = [](float n00, float n01, float n10, float n11) {
-      const float sx0 = __fadd_rn(n00, n01), sx1 = __fadd_rn(n10, n11);
-      const float sy0 = __fadd_rn(n00, n10), sy1 = __fadd_rn(n01, n11);
-      return make_float4(__fmul_rn(0.25f, __fadd_rn(sx0, sx1)), __fmul_rn(0.5f, __fsub_rn(sx1, sx0)),
-                         __fmul_rn(0.5f, __fsub_rn(sy1, sy0)), __fsub_rn(__fsub_rn(n11, n10), __fsub_rn(n01, n00)));
-    };
-    r[0] = coef(p0.x, p1.x, p2.x, p3.x);
-    r[1] = coef(p0.y, p1.y, p2.y, p3.y);
-    r[2] = coef(p0.z, p1.z, p2.z, p3.z);
-    r[3] = coef(q0.x, q1.x, q2.x, q3.x);
-    r[4] = coef(q0.y, q1.y, q2.y, q3.y);
-    r[5] = coef(q0.z, q1.z, q2.z, q3.z);
-#else
-    r[0] = make_float4(p0.x, p0.y, p0.z, q0.x);
-    r[1] = make_float4(q0.y, q0.z, p1.x, p1.y);
-    r[2] = make_float4(p1.z, q1.x, q1.y, q1.z);
-    r[3] = make_float4(p2.x, p2.y, p2.z, q2.x);
-    r[4] = make_float4(q2.y, q2.z, p3.x, p3.y);
-    r[5] = make_float4(p3.z, q3.x, q3.y, q3.z);
-#endif
+    cell_record(a, cx, cy);
+  }
+}
+
+// Gather records of cell rows [r0, r1) only.
+static __global__ void k_cell_records_rows(FieldParams<float> a, int r0, int r1) {
+  const int R = r1 - r0;
+  const long long n = (long long)a.mx * R;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int cx = (int)(k / R), cy = r0 + (int)(k - (long long)cx * R);
+    cell_record(a, cx, cy);
   }
 }
 

@@ -378,9 +378,17 @@ __global__ static void k_counts_own_rows(const int32_t* off, int64_t ncells, int
 }
 
 __global__ static void k_counts_band(int64_t n, const uint32_t* cell, int64_t base, int my, int32_t* counts) {
+  // The records of a cell are one run (the bands arrive in cell order): the
+  // run's first record adds -k and its last k + 1, so the count grows by the
+  // run's length with two atomics per cell instead of one per record. A run
+  // split in two (a record out of order) still adds both lengths.
+  auto key = [&](int64_t k) { const uint32_t w = cell[base + k]; return (int64_t)cw_ix(w) * my + cw_iy(w); };
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t w = cell[base + k];
-    atomicAdd(&counts[(int64_t)cw_ix(w) * my + cw_iy(w)], 1);
+    const int64_t c = key(k);
+    const bool first = k == 0 || key(k - 1) != c, last = k + 1 == n || key(k + 1) != c;
+    if (first && last) atomicAdd(&counts[c], 1);
+    else if (first) atomicAdd(&counts[c], (int32_t)-k);
+    else if (last) atomicAdd(&counts[c], (int32_t)(k + 1));
   }
 }
 

@@ -387,6 +387,24 @@ int nodes_and_field_energy(pbpic_handle* h, int row) {
   return PBPIC_OK;
 }
 
+// Node averages of node rows [b0, b1) and the gather records of the cells on
+// them (cell row c reads node rows c and c + 1), after some field rows changed.
+template <class T, bool MIXED>
+int node_rows(pbpic_handle* h, int b0, int b1) {
+  if (b1 <= b0) return PBPIC_OK;
+  FieldParams<T> a = field_params<T, MIXED>(h);
+  k_nodes_rows<T><<<grid_for((int64_t)(h->cfg.mx + 1) * (b1 - b0), 256), 256, 0, h->stream>>>(a, b0, b1);
+  CKLAUNCH("k_nodes_rows");
+  if constexpr (MIXED) {
+    const int r0 = std::max(0, b0 - 1), r1 = std::min(h->cfg.my, b1);
+    if (r1 > r0) {
+      k_cell_records_rows<<<grid_for((int64_t)h->cfg.mx * (r1 - r0), 256), 256, 0, h->stream>>>(a, r0, r1);
+      CKLAUNCH("k_cell_records_rows");
+    }
+  }
+  return PBPIC_OK;
+}
+
 template <class T, bool MIXED>
 int kinetic_row(pbpic_handle* h, int row) {
   TRY(ensure_hist(h, row + 1));
@@ -2577,7 +2595,15 @@ int do_field_rows(pbpic_handle* h, int j0, int nrows, void* buf, bool set) {
   if (set) {
     k_rows_set<T><<<g, 256, 0, h->stream>>>(p, h->cfg.mx, h->S, j0, nrows, (const T*)buf);
     CKLAUNCH("k_rows_set");
-    TRY((nodes_and_field_energy<T, MIXED>(h, h->itime)));
+    // Node row b averages field rows b - 1 and b, so the rows set feed node
+    // rows [j0, j0 + nrows]; with periodic y node row my repeats node row 0.
+    const int my = h->cfg.my;
+    const int b0 = std::max(0, (int)j0), b1 = std::min(my + 1, (int)(j0 + nrows + 1));
+    TRY((node_rows<T, MIXED>(h, b0, b1)));
+    if (h->cfg.ybc == PBPIC_BC_PERIODIC) {
+      if (b0 == 0) TRY((node_rows<T, MIXED>(h, my, my + 1)));
+      if (b1 == my + 1) TRY((node_rows<T, MIXED>(h, 0, 1)));
+    }
   } else {
     k_rows_get<T><<<g, 256, 0, h->stream>>>(p, h->cfg.mx, h->S, j0, nrows, (T*)buf);
     CKLAUNCH("k_rows_get");
