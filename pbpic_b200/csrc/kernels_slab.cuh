@@ -203,28 +203,45 @@ __device__ __forceinline__ int column_of(const int32_t* start, int mx, int64_t k
   return lo;
 }
 
+// One 32-byte reference record with two 16-byte stores when the buffer is
+// 16-byte aligned (FP64 records, 56 bytes, are stored as they are).
+__device__ __forceinline__ void store_record(RefRec<float>* p, const RefRec<float>& r, bool al16) {
+  if (al16) {
+    uint4* d = reinterpret_cast<uint4*>(p);
+    d[0] = make_uint4(__float_as_uint(r.dx), __float_as_uint(r.dy), __float_as_uint(r.ux), __float_as_uint(r.uy));
+    d[1] = make_uint4(__float_as_uint(r.uz), (unsigned)r.grid, (unsigned)r.q, (unsigned)r.pid);
+  } else {
+    *p = r;
+  }
+}
+__device__ __forceinline__ void store_record(RefRec<double>* p, const RefRec<double>& r, bool) { *p = r; }
+
 // Band extraction from sorted particles: output k of column ix comes from
-// off[ix*my + y_lo] + (k - colstart[ix]); same records as k_band_out.
+// off[ix*my + y_lo] + (k - colstart[ix]); same records as k_band_out. One
+// block per column (grid-stride over the columns).
 template <class T, class R>
-__global__ void k_band_out_sorted(int64_t total, const int32_t* colstart, const int32_t* off, int mx, int my, int y_lo,
+__global__ void k_band_out_sorted(const int32_t* colstart, const int32_t* off, int mx, int my, int y_lo,
                                   const uint32_t* cell, const T* dx, const T* dy, const T* ux, const T* uy,
                                   const T* uz, const int32_t* pid, int my_global, int row_offset, RefRec<R>* out,
-                                  const int32_t* perm) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = column_of(colstart, mx, k);
-    const int64_t j = (int64_t)off[(int64_t)ix * my + y_lo] + (k - colstart[ix]);  // sorted position
-    const int64_t i = perm ? (int64_t)perm[j] : j;
-    const uint32_t w = cell[i];
-    RefRec<R> r;
-    r.dx = (R)dx[i];
-    r.dy = (R)dy[i];
-    r.ux = (R)ux[i];
-    r.uy = (R)uy[i];
-    r.uz = (R)uz[i];
-    r.grid = my_global * cw_ix(w) + cw_iy(w) + row_offset + 1;
-    r.q = cw_sp(w) ? -1 : 1;
-    r.pid = pid ? pid[i] : 0;
-    out[k] = r;
+                                  const int32_t* perm, bool al16) {
+  for (int ix = blockIdx.x; ix < mx; ix += gridDim.x) {
+    const int64_t k0 = colstart[ix], k1 = colstart[ix + 1];
+    const int64_t j0 = (int64_t)off[(int64_t)ix * my + y_lo] - k0;  // sorted position of output k: j0 + k
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+      const int64_t j = j0 + k;
+      const int64_t i = perm ? (int64_t)perm[j] : j;
+      const uint32_t w = cell[i];
+      RefRec<R> r;
+      r.dx = (R)dx[i];
+      r.dy = (R)dy[i];
+      r.ux = (R)ux[i];
+      r.uy = (R)uy[i];
+      r.uz = (R)uz[i];
+      r.grid = my_global * cw_ix(w) + cw_iy(w) + row_offset + 1;
+      r.q = cw_sp(w) ? -1 : 1;
+      r.pid = pid ? pid[i] : 0;
+      store_record(out + k, r, al16);
+    }
   }
 }
 

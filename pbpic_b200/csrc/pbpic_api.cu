@@ -2390,10 +2390,10 @@ int band_extract_sorted(pbpic_handle* h, int y_lo, int y_hi, int my_global, int 
   if (total > 0 && !dst) return fail(PBPIC_EINVAL, "null band destination");
   const int b = h->cur;
   if (total > 0) {
-    k_band_out_sorted<T, T><<<grid_for(total, 256), 256, 0, s>>>(
-        total, colstart, h->off, mx, h->cfg.my, y_lo, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
+    k_band_out_sorted<T, T><<<std::min(mx, 148 * 16), 256, 0, s>>>(
+        colstart, h->off, mx, h->cfg.my, y_lo, h->cell[b], P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
         P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b], my_global, row_offset, (RefRec<T>*)dst,
-        h->lazy ? h->perm : nullptr);
+        h->lazy ? h->perm : nullptr, ((uintptr_t)dst & 15) == 0);
     CKLAUNCH("k_band_out_sorted");
   }
   CK(cudaStreamSynchronize(s));
