@@ -152,13 +152,30 @@ __device__ __forceinline__ void st4(uint32_t* p, const uint32_t (&v)[4]) {
 // Reciprocal square root and quotient of the push. Plain form, exact order
 // (COMPAT instances): correctly rounded square roots and quotients, as the
 // reference's expressions. Plain form otherwise: 1/gamma from CUDA's double
-// rsqrt, so that the push's chain holds one FP64 division instead of four
-// quotients and two square roots (results within a few ulp of the exact
-// order). Mixed form: the hardware reciprocal square root and fast division
-// (deterministic, about 2 ulp).
+// rsqrt and the rotation's 2/(1 + t^2) by Newton steps from the hardware
+// reciprocal estimate (push_two_over), so that the push's chain holds no FP64
+// division instead of four quotients and two square roots (results within a
+// few ulp of the exact order). Mixed form: the hardware reciprocal square root
+// and fast division (deterministic, about 2 ulp).
 __device__ __forceinline__ float push_rsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double push_rsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float push_fdiv(float a, float b) { return __fdividef(a, b); }
+
+// Plain form, fast mode: 2/x for x = 1 + |t|^2 >= 1 by Newton-Raphson
+// refinement of the hardware reciprocal estimate (rcp.approx.ftz.f64): two
+// steps y <- y + y (1 - x y), each squaring the relative error, then one
+// residual correction of the quotient, q <- q + (2 - x q) y (Markstein's
+// correction); a few ulp from the correctly rounded quotient at most.
+__device__ __forceinline__ double push_two_over(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = __fma_rn(-x, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-x, y, 1.0);
+  y = __fma_rn(y, e, y);
+  const double q = __dmul_rn(2.0, y);
+  return __fma_rn(__fma_rn(-x, q, 2.0), y, q);
+}
 
 // Outcome of pushing one particle.
 template <class T>
@@ -249,6 +266,8 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
   const T tsq1 = A::mad(tz, tz, A::mad(ty, ty, A::mad(tx, tx, one)));
   if constexpr (MIXED) {
     t2 = push_fdiv(T(2), tsq1);
+  } else if constexpr (!COMPAT) {
+    t2 = push_two_over(tsq1);
   } else {
     t2 = A::div(T(2), tsq1);
   }
@@ -387,16 +406,17 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
 
   // ---- boundaries: x periodic (pic2d.f90:1032); y periodic (the 1-rank
   // exchange of pic2d.f90:1033-1146 reduces to a wrap) or specular walls.
-  int nix = ix + dcx;
-  nix = nix < 0 ? nix + a.mx : (nix >= a.mx ? nix - a.mx : nix);
-  int niy = iy + dcy;
+  int nix = ix + dcx, niy = iy + dcy;
   T ruy = uy, rdy = dy2;
-  if (a.ybc == 0) {
-    niy = niy < 0 ? niy + a.my : (niy >= a.my ? niy - a.my : niy);
-  } else if (niy < 0 || niy >= a.my) {
-    niy = niy < 0 ? 0 : a.my - 1;
-    rdy = -dy2;
-    ruy = -uy;
+  if ((unsigned)nix >= (unsigned)a.mx || (unsigned)niy >= (unsigned)a.my) {  // a particle leaving the domain
+    nix = nix < 0 ? nix + a.mx : (nix >= a.mx ? nix - a.mx : nix);
+    if (a.ybc == 0) {
+      niy = niy < 0 ? niy + a.my : (niy >= a.my ? niy - a.my : niy);
+    } else if (niy < 0 || niy >= a.my) {
+      niy = niy < 0 ? 0 : a.my - 1;
+      rdy = -dy2;
+      ruy = -uy;
+    }
   }
   o.cw = cw_make(nix, niy, sp);
   o.dx = dx2;
