@@ -110,6 +110,12 @@ __device__ __forceinline__ void load_coef(const float* r, CellCoef& c) {
 #pragma unroll
   for (int k = 0; k < 6; ++k) c.f[k] = __ldg(q + k);
 }
+// The same from the tile's records staged in shared memory.
+__device__ __forceinline__ void load_coef_staged(const float* r, CellCoef& c) {
+  const float4* q = reinterpret_cast<const float4*>(r);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) c.f[k] = q[k];
+}
 __device__ __forceinline__ float coef_at(const float4& q, float x, float y) {
   return __fmaf_rn(__fmaf_rn(q.w, x, q.z), y, __fmaf_rn(q.y, x, q.x));
 }
@@ -147,6 +153,40 @@ __device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
 }
 __device__ __forceinline__ void st4(uint32_t* p, const uint32_t (&v)[4]) {
   *reinterpret_cast<uint4*>(p) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+// Bulk copy of a tile's gather records into shared memory (the copy engine's
+// cp.async.bulk, completion counted on an mbarrier; no multicast). The wait
+// is bounded: a copy that has not landed after PUSH_WAIT_TRIES polls raises
+// PBPIC_STATUS_COPY_TIMEOUT and the push reads the records from global memory.
+#ifndef PBPIC_PUSH_STAGE_RECS
+#define PBPIC_PUSH_STAGE_RECS 1
+#endif
+constexpr int PUSH_WAIT_TRIES = 1 << 22;
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(b)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* b) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of dst come first
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(b))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+  for (int i = 0; i < PUSH_WAIT_TRIES; ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
 }
 
 // Reciprocal square root and quotient of the push. Plain form, exact order
@@ -565,12 +605,14 @@ template <class T, bool MIXED>
 struct PushSmem {
   T stage[PushThreads<T>::value / 32][17][33];
   double red[32];
+  uint64_t mbar;
 };
 template <>
 struct PushSmem<float, true> {
   float stage[PushThreads<float>::value / 32][17][33];
   float first[PushThreads<float>::value / 32][17][33];
   double red[32];
+  uint64_t mbar;  // completion of the tile records' bulk copy (tile_begin)
 };
 
 // Rare path: a particle outside its tile adds its 16 terms (staged in the
@@ -637,14 +679,24 @@ struct TileWin {
   int* hist;
   unsigned* clo;  // crossers: jx, jy planes (8 * WR)
   int* chi;
+  const float* rec;  // mixed form: the tile's gather records (rows y0..y1-1), staged in shared memory
+  uint64_t* mbar;    // completion of the records' bulk copy
 };
+
+// Byte offset of the mixed form's staged records (after the split windows) and
+// of their mbarrier (after the records of a 64-row tile).
+__host__ __device__ __forceinline__ size_t push_rec_offset(int ty) {
+  return ((size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4 + 15) & ~(size_t)15;
+}
+
 
 // Clears the windows of tile t and starts its histogram from the input's cell
 // counts: the input is sorted by cell, so every particle of a tile cell stays
 // in that cell's bin unless it crosses, and each crossing particle moves one
 // count.
 template <class T, bool MIXED, bool HIST>
-__device__ __forceinline__ TileWin<T, MIXED> tile_begin(const PushParams<T>& a, int t, unsigned char* smem_raw) {
+__device__ __forceinline__ TileWin<T, MIXED> tile_begin(const PushParams<T>& a, int t, unsigned char* smem_raw,
+                                                        uint64_t* mbar) {
   using Acc = typename TileWin<T, MIXED>::Acc;
   TileWin<T, MIXED> w;
   w.TY = a.tile_rows;
@@ -657,6 +709,14 @@ __device__ __forceinline__ TileWin<T, MIXED> tile_begin(const PushParams<T>& a, 
   w.ixt = t / a.tiles_per_col;
   w.y0 = (t - w.ixt * a.tiles_per_col) * w.TY;
   w.y1 = min(w.y0 + w.TY, a.my);
+  w.rec = reinterpret_cast<const float*>(smem_raw + push_rec_offset(w.TY));
+  w.mbar = mbar;
+  if constexpr (MIXED && PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS) {
+    // the records of cells (ixt, y0..y1-1) are contiguous: one copy of 96 B per row
+    if (threadIdx.x == 0)
+      bulk_load(const_cast<float*>(w.rec), a.cg + ((long long)w.ixt * a.my + w.y0) * 24, (unsigned)(w.y1 - w.y0) * 96u,
+                w.mbar);
+  }
   for (int e = threadIdx.x; e < 16 * w.WR; e += blockDim.x) w.win[e] = Acc(0);
   if (MIXED)
     for (int e = threadIdx.x; e < 8 * w.WR; e += blockDim.x) {
@@ -792,12 +852,17 @@ __device__ __forceinline__ void tile_end(const PushParams<T>& a, int t, const Ti
 
 // Push of tile t of the domain `a`, by all threads of the block: G float4
 // groups of particles per thread per pass (8 particles for G = 2).
+// parity: the phase of sm.mbar this tile's record copy completes (the
+// block's count of earlier tiles, mod 2).
 template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true, bool GATHER = false>
 __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
-                                          unsigned char* smem_raw) {
+                                          unsigned char* smem_raw, unsigned parity) {
   constexpr int PT = 4 * G;  // particles per thread per pass
-  const TileWin<T, MIXED> tw = tile_begin<T, MIXED, HIST>(a, t, smem_raw);
+  constexpr bool STAGED = MIXED && PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS;
+  const TileWin<T, MIXED> tw = tile_begin<T, MIXED, HIST>(a, t, smem_raw, &sm.mbar);
   const int TY = tw.TY, WR = tw.WR, ixt = tw.ixt, y0 = tw.y0, y1 = tw.y1;
+  bool staged = false;  // this thread reads the tile's records from shared memory
+  if constexpr (STAGED) staged = mbar_wait(tw.mbar, parity);
   auto* win = tw.win;
   unsigned* clo = tw.clo;
   int* chi = tw.chi;
@@ -816,6 +881,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
   T* mycol = &sm.stage[w][0][lane];
   double ke_e = 0.0, ke_i = 0.0;
   int status = 0;
+  if (STAGED && !staged) status |= PBPIC_STATUS_COPY_TIMEOUT;
   for (int q0 = pbeg & ~3; q0 < pend; q0 += PT * PushThreads<T>::value) {
     // thread-level accumulation of the stencils of particles sharing a cell
     T acc[17];
@@ -896,7 +962,11 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
         const int cid = (ix << 16) | iy;
         if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
-          if constexpr (MIXED && PBPIC_CELL_COEF) {
+          if constexpr (STAGED) {
+            const int r = iy - y0;
+            if (staged && ix == ixt && (unsigned)r < (unsigned)(y1 - y0)) load_coef_staged(tw.rec + r * 24, cc);
+            else load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
+          } else if constexpr (MIXED && PBPIC_CELL_COEF) {
             load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
           } else if constexpr (MIXED) {
             load_cell(a.cg + ((long long)ix * a.my + iy) * 24, n00, n01, n10, n11);
@@ -1049,6 +1119,9 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     ke_i += (double)pke_i;
     pass_sums<T, MIXED>([&](int k) { return acc[k]; }, acc_key, first_key, sm.stage[w], fw, win, WR, sc, sx, sy);
   }
+  // a copy that did not land in time must not be in flight when the block
+  // moves on: wait for it again (bounded) before the shared memory is reused
+  if (STAGED && !staged) mbar_wait(tw.mbar, parity);
   tile_end<T, MIXED, HIST>(a, t, tw, ke_e, ke_i, status, sm.red);
 }
 
@@ -1059,7 +1132,9 @@ template <class T, bool MIXED, bool HIST, bool COMPAT, bool GATHER = false>
 __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINBLOCKS : PBPIC_PUSH_MINBLOCKS_FP64) k_push(PushParams<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PushSmem<T, MIXED> sm;
-  push_tile<T, MIXED, HIST, MIXED ? PBPIC_PUSH_HALVES : PBPIC_PUSH_HALVES_FP64, COMPAT, GATHER>(a, blockIdx.x, sm, smem_raw);
+  if (threadIdx.x == 0) mbar_init(&sm.mbar);  // thread 0 also starts the copy; the others wait after a barrier
+  push_tile<T, MIXED, HIST, MIXED ? PBPIC_PUSH_HALVES : PBPIC_PUSH_HALVES_FP64, COMPAT, GATHER>(a, blockIdx.x, sm,
+                                                                                              smem_raw, 0u);
 }
 
 // Batched domains: persistent blocks take (domain, tile) pairs from a global
@@ -1071,6 +1146,8 @@ __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINB
   __shared__ PushSmem<T, MIXED> sm;
   __shared__ PushParams<T> a;
   __shared__ int next;
+  if (threadIdx.x == 0) mbar_init(&sm.mbar);
+  unsigned parity = 0;
   while (true) {
     if (threadIdx.x == 0) next = atomicAdd(counter, 1);
     __syncthreads();
@@ -1079,7 +1156,8 @@ __global__ void __launch_bounds__(PushThreads<T>::value, MIXED ? PBPIC_PUSH_MINB
     const int2 it = tiles[t];
     if (threadIdx.x == 0) a = descs[it.x];
     __syncthreads();
-    push_tile<T, MIXED, HIST, G, COMPAT, GATHER>(a, it.y, sm, smem_raw);
+    push_tile<T, MIXED, HIST, G, COMPAT, GATHER>(a, it.y, sm, smem_raw, parity);
+    parity ^= 1u;
     __syncthreads();
   }
 }

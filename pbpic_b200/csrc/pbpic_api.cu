@@ -220,12 +220,14 @@ int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
 
 // Dynamic shared memory of k_push: the tile's current window (16 x (ty+3)
 // 8-byte accumulators), the new-cell histogram (3 x (ty+2) int) and, in the
-// mixed form, the crossers' split 32-bit windows (2 x 8 x (ty+3)); with the
-// static part this stays below the 48 KB a launch gets without opting in. The
+// mixed form, the crossers' split 32-bit windows (2 x 8 x (ty+3)) and the
+// tile's gather records staged by a bulk copy (96 B a row); with the static
+// part this stays below the 48 KB a launch gets without opting in. The
 // plain form adds the second stage of its run sums (a warp's 17 x 33 doubles
 // per warp), which takes 256-thread blocks above 48 KB (push_smem_optin).
 size_t push_smem_bytes(int ty, bool mixed) {
   if (!mixed) return push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * sizeof(double);
+  if (PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS) return push_rec_offset(ty) + (size_t)ty * 96;  // + staged records
   return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4;
 }
 
