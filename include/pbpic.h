@@ -52,7 +52,7 @@ extern "C" {
 #define PBPIC_STATUS_NAN 2       /* a momentum became NaN or infinite */
 #define PBPIC_STATUS_UNSORTED 4  /* a push met a particle outside its tile (informational) */
 #define PBPIC_STATUS_BAD_RECORD 8   /* a band record fell outside this domain's rows (pbpic_band_replace) */
-#define PBPIC_STATUS_COPY_TIMEOUT 16 /* a push's bulk copy of a tile's gather records did not land within its bounded wait (the push then read them from global memory) */
+#define PBPIC_STATUS_COPY_TIMEOUT 16 /* a push's bulk copy of a tile's gather records or node columns did not land within its bounded wait (the push then read them from global memory) */
 
 typedef struct pbpic_config {
   int32_t mx, my;      /* cells in x and y (nx, ny of pic2d.f90:12; one domain) */

@@ -95,6 +95,12 @@ __device__ __forceinline__ Node6<double> load_node(const double* g) {
   return Node6<double>{a.x, a.y, b.x, c.x, c.y, d.x};
 }
 
+__device__ __forceinline__ Node6<double> load_node_staged(const double* g) {
+  const double2* p = reinterpret_cast<const double2*>(g);
+  const double2 a = p[0], b = p[1], c = p[2], d = p[3];
+  return Node6<double>{a.x, a.y, b.x, c.x, c.y, d.x};
+}
+
 // Mixed form: a cell's gather record (k_cell_records) holds, per field (ex ey
 // ez bx by bz, one aligned 16-byte group each), the bilinear coefficients
 // (A, B, C, D) of the field over the cell, f(x, y) = A + B x + C y + D x y for
@@ -155,12 +161,16 @@ __device__ __forceinline__ void st4(uint32_t* p, const uint32_t (&v)[4]) {
   *reinterpret_cast<uint4*>(p) = make_uint4(v[0], v[1], v[2], v[3]);
 }
 
-// Bulk copy of a tile's gather records into shared memory (the copy engine's
-// cp.async.bulk, completion counted on an mbarrier; no multicast). The wait
-// is bounded: a copy that has not landed after PUSH_WAIT_TRIES polls raises
-// PBPIC_STATUS_COPY_TIMEOUT and the push reads the records from global memory.
+// Bulk copy of a tile's gather records (mixed form) or node-grid columns
+// (plain form) into shared memory (the copy engine's cp.async.bulk,
+// completion counted on an mbarrier; no multicast). The wait is bounded: a
+// copy that has not landed after PUSH_WAIT_TRIES polls raises
+// PBPIC_STATUS_COPY_TIMEOUT and the push reads global memory instead.
 #ifndef PBPIC_PUSH_STAGE_RECS
 #define PBPIC_PUSH_STAGE_RECS 1
+#endif
+#ifndef PBPIC_PUSH_STAGE_NODES
+#define PBPIC_PUSH_STAGE_NODES 1  // plain form: the tile's two node-grid columns
 #endif
 constexpr int PUSH_WAIT_TRIES = 1 << 22;
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -168,9 +178,13 @@ __device__ __forceinline__ void mbar_init(uint64_t* b) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(b)) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* b) {
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of dst come first
+// Announces `bytes` of bulk copies on mbarrier b (after the block's earlier
+// reads of the destination, ordered by a barrier, and this fence).
+__device__ __forceinline__ void bulk_expect(uint64_t* b, unsigned bytes) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* b) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                    smem_addr(dst)),
                "l"(src), "r"(bytes), "r"(smem_addr(b))
@@ -679,14 +693,19 @@ struct TileWin {
   int* hist;
   unsigned* clo;  // crossers: jx, jy planes (8 * WR)
   int* chi;
-  const float* rec;  // mixed form: the tile's gather records (rows y0..y1-1), staged in shared memory
-  uint64_t* mbar;    // completion of the records' bulk copy
+  const T* stg;    // staged in shared memory: the mixed form's gather records of rows y0..y1-1 (24 values
+                   // a row), the plain form's node-grid columns ixt and ixt+1 of rows y0..y1 (8 a node)
+  uint64_t* mbar;  // completion of their bulk copy
 };
 
 // Byte offset of the mixed form's staged records (after the split windows) and
 // of their mbarrier (after the records of a 64-row tile).
 __host__ __device__ __forceinline__ size_t push_rec_offset(int ty) {
   return ((size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4 + 15) & ~(size_t)15;
+}
+// ... and of the plain form's staged node columns (after its second stage).
+__host__ __device__ __forceinline__ size_t push_node_offset(int ty) {
+  return (push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * 8 + 15) & ~(size_t)15;
 }
 
 
@@ -709,13 +728,24 @@ __device__ __forceinline__ TileWin<T, MIXED> tile_begin(const PushParams<T>& a, 
   w.ixt = t / a.tiles_per_col;
   w.y0 = (t - w.ixt * a.tiles_per_col) * w.TY;
   w.y1 = min(w.y0 + w.TY, a.my);
-  w.rec = reinterpret_cast<const float*>(smem_raw + push_rec_offset(w.TY));
+  w.stg = reinterpret_cast<const T*>(smem_raw + (MIXED ? push_rec_offset(w.TY) : push_node_offset(w.TY)));
   w.mbar = mbar;
   if constexpr (MIXED && PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS) {
     // the records of cells (ixt, y0..y1-1) are contiguous: one copy of 96 B per row
-    if (threadIdx.x == 0)
-      bulk_load(const_cast<float*>(w.rec), a.cg + ((long long)w.ixt * a.my + w.y0) * 24, (unsigned)(w.y1 - w.y0) * 96u,
-                w.mbar);
+    if (threadIdx.x == 0) {
+      const unsigned bytes = (unsigned)(w.y1 - w.y0) * 96u;
+      bulk_expect(w.mbar, bytes);
+      bulk_copy(const_cast<T*>(w.stg), a.cg + ((long long)w.ixt * a.my + w.y0) * 24, bytes, w.mbar);
+    }
+  } else if constexpr (!MIXED && PBPIC_PUSH_STAGE_NODES) {
+    // nodes (ixt, y0..y1) and (ixt+1, y0..y1): two contiguous runs of 64 B per node
+    if (threadIdx.x == 0) {
+      const unsigned bytes = (unsigned)(w.y1 - w.y0 + 1) * 64u;
+      const T* g = a.ng + ((long long)w.ixt * (a.my + 1) + w.y0) * 8;
+      bulk_expect(w.mbar, 2 * bytes);
+      bulk_copy(const_cast<T*>(w.stg), g, bytes, w.mbar);
+      bulk_copy(const_cast<T*>(w.stg) + (w.TY + 1) * 8, g + (long long)(a.my + 1) * 8, bytes, w.mbar);
+    }
   }
   for (int e = threadIdx.x; e < 16 * w.WR; e += blockDim.x) w.win[e] = Acc(0);
   if (MIXED)
@@ -858,7 +888,7 @@ template <class T, bool MIXED, bool HIST, int G, bool COMPAT = true, bool GATHER
 __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, PushSmem<T, MIXED>& sm,
                                           unsigned char* smem_raw, unsigned parity) {
   constexpr int PT = 4 * G;  // particles per thread per pass
-  constexpr bool STAGED = MIXED && PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS;
+  constexpr bool STAGED = MIXED ? (PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS) : PBPIC_PUSH_STAGE_NODES;
   const TileWin<T, MIXED> tw = tile_begin<T, MIXED, HIST>(a, t, smem_raw, &sm.mbar);
   const int TY = tw.TY, WR = tw.WR, ixt = tw.ixt, y0 = tw.y0, y1 = tw.y1;
   bool staged = false;  // this thread reads the tile's records from shared memory
@@ -962,14 +992,22 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
         const int cid = (ix << 16) | iy;
         if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
-          if constexpr (STAGED) {
+          if constexpr (MIXED && STAGED) {
             const int r = iy - y0;
-            if (staged && ix == ixt && (unsigned)r < (unsigned)(y1 - y0)) load_coef_staged(tw.rec + r * 24, cc);
+            if (staged && ix == ixt && (unsigned)r < (unsigned)(y1 - y0)) load_coef_staged(tw.stg + r * 24, cc);
             else load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
           } else if constexpr (MIXED && PBPIC_CELL_COEF) {
             load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
           } else if constexpr (MIXED) {
             load_cell(a.cg + ((long long)ix * a.my + iy) * 24, n00, n01, n10, n11);
+          } else if (STAGED && staged && ix == ixt && (unsigned)(iy - y0) < (unsigned)(y1 - y0)) {
+            // FP64 from the tile's staged node columns
+            const T* s00 = tw.stg + (iy - y0) * 8;
+            const T* s10 = s00 + (TY + 1) * 8;
+            n00 = load_node_staged(s00);
+            n01 = load_node_staged(s00 + 8);
+            n10 = load_node_staged(s10);
+            n11 = load_node_staged(s10 + 8);
           } else {  // FP64: from the node grid (its records took more registers than they saved)
             const T* g00 = a.ng + ((long long)ix * (a.my + 1) + iy) * 8;
             const T* g10 = g00 + (long long)(a.my + 1) * 8;

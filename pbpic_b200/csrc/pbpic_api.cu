@@ -226,7 +226,10 @@ int64_t plane_elems(const pbpic_handle* h) { return (int64_t)h->cfg.mx * h->S; }
 // plain form adds the second stage of its run sums (a warp's 17 x 33 doubles
 // per warp), which takes 256-thread blocks above 48 KB (push_smem_optin).
 size_t push_smem_bytes(int ty, bool mixed) {
-  if (!mixed) return push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * sizeof(double);
+  if (!mixed) {
+    if (PBPIC_PUSH_STAGE_NODES) return push_node_offset(ty) + (size_t)2 * (ty + 1) * 64;  // + staged node columns
+    return push_first_offset(ty) + (size_t)(PushThreads<double>::value / 32) * 17 * 33 * sizeof(double);
+  }
   if (PBPIC_CELL_COEF && PBPIC_PUSH_STAGE_RECS) return push_rec_offset(ty) + (size_t)ty * 96;  // + staged records
   return (size_t)16 * (ty + 3) * 8 + (size_t)3 * (ty + 2) * 4 + (size_t)16 * (ty + 3) * 4;
 }
