@@ -37,7 +37,7 @@ METRIC = "particle-steps/s on 1 B200: FP32 mixed vs FP64 plain at stated energy 
 # state read through the sort's permutation, the permutation itself, the state written in cell
 # order), from the ncu capture of the 512x256 sheet summarised in
 # profiles/k_push_fp32_harris_512x256_ppc100.txt; traffic grows in proportion to the particles.
-PUSH_DRAM_BYTES_PER_PARTICLE = 61.0
+PUSH_DRAM_BYTES_PER_PARTICLE = 61.2
 PUSH_KERNEL = "k_push<float,true,true,false,true>"
 UNIT = "particle-steps/s"
 

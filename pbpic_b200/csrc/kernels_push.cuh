@@ -375,7 +375,16 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
 
   // ---- charge-conserving deposit terms (pic2d.f90:1237-1295), indices
   // relative to the old cell: i1 = j1 = 0, i2 = dcx, j2 = dcy.
-  const T qx = PBD_SPECIES(a.qx, sp), qy = PBD_SPECIES(a.qy, sp), qq = PBD_SPECIES(a.q, sp);
+  T qx, qy, qq;
+  if constexpr (MIXED) {  // the mixed form's charges are the unit charges: +1 ion, -1 electron (the sign bit)
+    qq = __uint_as_float(0x3f800000u | ((unsigned)sp << 31));
+    qx = qq;
+    qy = qq;
+  } else {
+    qx = PBD_SPECIES(a.qx, sp);
+    qy = PBD_SPECIES(a.qy, sp);
+    qq = PBD_SPECIES(a.q, sp);
+  }
   T im, jm;
   if constexpr (MIXED || !COMPAT) {  // cell-relative form (the plain form's exact order below)
     // Positions in cell units from the old cell's lower-left node: start
@@ -942,15 +951,14 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {  // the input is not written by this launch: read-only loads
-          const int p = q + j;
-          const bool act = p >= pbeg && p < pend;
+          // (a position outside the tile has entry 0: element 0 is read and its values are not used)
           const int e = sidx[j];
-          cw[j] = act ? __ldg(a.cell + e) : 0u;
-          px[j] = act ? __ldg(a.dx + e) : T(0);
-          py[j] = act ? __ldg(a.dy + e) : T(0);
-          pux[j] = act ? __ldg(a.ux + e) : T(0);
-          puy[j] = act ? __ldg(a.uy + e) : T(0);
-          puz[j] = act ? __ldg(a.uz + e) : T(0);
+          cw[j] = __ldg(a.cell + e);
+          px[j] = __ldg(a.dx + e);
+          py[j] = __ldg(a.dy + e);
+          pux[j] = __ldg(a.ux + e);
+          puy[j] = __ldg(a.uy + e);
+          puz[j] = __ldg(a.uz + e);
         }
       } else if (full) {
         ld4(a.cell + q, cw);
@@ -979,7 +987,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
 #endif
       for (int j = 0; j < 4; ++j) {
         const int p = q + j;
-        if (p < pbeg || p >= pend) {
+        if (!full && (p < pbeg || p >= pend)) {
           rot4(cw, cw[0]);
           rot4(px, px[0]);
           rot4(py, py[0]);
@@ -991,16 +999,17 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         const uint32_t wrd = cw[0];
         const int sp = cw_sp(wrd), ix = cw_ix(wrd), iy = cw_iy(wrd);
         const int cid = (ix << 16) | iy;
+        const bool inwin = ix == ixt && (unsigned)(iy - y0) < (unsigned)(y1 - y0);  // in this tile (sorted input)
         if (!PBPIC_PUSH_NODECACHE || cid != cache_cell) {
           if constexpr (MIXED && STAGED) {
             const int r = iy - y0;
-            if (staged && ix == ixt && (unsigned)r < (unsigned)(y1 - y0)) load_coef_staged(tw.stg + r * 24, cc);
+            if (staged && inwin) load_coef_staged(tw.stg + r * 24, cc);
             else load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
           } else if constexpr (MIXED && PBPIC_CELL_COEF) {
             load_coef(a.cg + ((long long)ix * a.my + iy) * 24, cc);
           } else if constexpr (MIXED) {
             load_cell(a.cg + ((long long)ix * a.my + iy) * 24, n00, n01, n10, n11);
-          } else if (STAGED && staged && ix == ixt && (unsigned)(iy - y0) < (unsigned)(y1 - y0)) {
+          } else if (STAGED && staged && inwin) {
             // FP64 from the tile's staged node columns
             const T* s00 = tw.stg + (iy - y0) * 8;
             const T* s10 = s00 + (TY + 1) * 8;
@@ -1024,7 +1033,6 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
         else
           push_one<T, MIXED, COMPAT>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
         status |= o.status;
-        const bool inwin = ix == ixt && iy >= y0 && iy < y1;
         const bool cross = o.dcx != 0 || o.dcy != 0;
         if (HIST && cross && inwin) status |= hist_move<T, MIXED>(a, tw, wrd, &o.cw, o.dcx, ix, iy);
         if (inwin) {
