@@ -244,6 +244,7 @@ struct Pushed {
   // the outer product of the x and y midpoint weights (1-zdx at 0, zdx at
   // di; 1-zdy at 0, zdy at dj)
   T ja, jw, jb, jv, quz, zdx, zdy;
+  T q, rw[4];            // charge and the rho weights of e[12..15] (e[12 + k] = q * rw[k])
   T ke;                  // kinetic energy (gamma - 1) ms
   int status;
 };
@@ -465,6 +466,11 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
     o.e[13] = A::mul(r2, qq);  // rho (1, 0)
     o.e[14] = A::mul(r3, qq);  // rho (0, 1)
     o.e[15] = A::mul(r1, qq);  // rho (1, 1)
+    o.q = qq;
+    o.rw[0] = r4;
+    o.rw[1] = r2;
+    o.rw[2] = r3;
+    o.rw[3] = r1;
   }
 
   // ---- boundaries: x periodic (pic2d.f90:1032); y periodic (the 1-rank
@@ -926,6 +932,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     T acc[17];
 #pragma unroll
     for (int k = 0; k < 17; ++k) acc[k] = T(0);
+    auto sval = [&](int k) -> T { return acc[k]; };  // stencil entry k of the thread's sums
     int acc_key = -1;
     int first_key = -1;  // cell of this pass's finished first part (in `fw`), or -1
     int cache_cell = -1;
@@ -1043,14 +1050,14 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
                 first_key = acc_key;
 #pragma unroll
                 for (int k = 0; k < 17; ++k) {
-                  fw[k * 33 + lane] = acc[k];
+                  fw[k * 33 + lane] = sval(k);
                   acc[k] = T(0);
                 }
               }
               if (acc_key >= 0 && acc_key != first_key) {  // a cell wholly inside this thread's pass
 #pragma unroll
                 for (int k = 0; k < 17; ++k) {
-                  mycol[k * 33] = acc[k];
+                  mycol[k * 33] = sval(k);
                   acc[k] = T(0);
                 }
                 flush_column<T, MIXED>(win, mycol, acc_key, WR);
@@ -1095,10 +1102,16 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
             acc[4 + 7] += zxp * o.e[9];
             acc[4 + 8] += zxp * zyp * o.e[11];
           }
-          acc[13] += o.e[12];
-          acc[14] += o.e[13];
-          acc[15] += o.e[14];
-          acc[16] += o.e[15];
+          if constexpr (MIXED) {  // unit charge: q * w + acc in one rounding, the same as acc + (q * w)
+            using F = M<T, true>;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[13 + k] = F::mad(o.q, o.rw[k], acc[13 + k]);
+          } else {
+            acc[13] += o.e[12];
+            acc[14] += o.e[13];
+            acc[15] += o.e[14];
+            acc[16] += o.e[15];
+          }
           if (cross) {  // second zig-zag segment, attached to the new cell
             const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
             const int b0 = (JX * 4 + wx) * WR + wy, b1 = (JY * 4 + wx) * WR + wy;
@@ -1163,7 +1176,7 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
     }
     ke_e += (double)pke_e;
     ke_i += (double)pke_i;
-    pass_sums<T, MIXED>([&](int k) { return acc[k]; }, acc_key, first_key, sm.stage[w], fw, win, WR, sc, sx, sy);
+    pass_sums<T, MIXED>(sval, acc_key, first_key, sm.stage[w], fw, win, WR, sc, sx, sy);
   }
   // a copy that did not land in time must not be in flight when the block
   // moves on: wait for it again (bounded) before the shared memory is reused
