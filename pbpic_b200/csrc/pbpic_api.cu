@@ -163,6 +163,9 @@ struct pbpic_handle {
   bool sorted = false;
   bool fused_ok = false;    // grid admits the fused counting sort (distinct window cells)
   bool hist_valid = false;  // the last push counted new cells per tile on a sorted array
+  bool defer_sort = false;  // pbpic_step: the push leaves its fused sort to run beside the field solve
+  cudaStream_t side = nullptr;                       // pbpic_step: the field solve's stream
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // pbpic_step: push -> field solve, field solve -> next
   // The fused sort leaves the particle data in place and writes perm (sorted
   // position -> element); while `lazy`, the cell order is the arrays read
   // through perm. The next push reads through it; every other reader of the
@@ -561,7 +564,7 @@ int do_push(pbpic_handle* h) {
   CKLAUNCH("k_energy_row");
   h->hist_valid = hist;
   h->sorted = false;
-  if (autosort) TRY((do_fused_sort<T, MIXED>(h)));
+  if (autosort && !h->defer_sort) TRY((do_fused_sort<T, MIXED>(h)));
   return PBPIC_OK;
 }
 
@@ -660,6 +663,46 @@ int do_fieldsolve(pbpic_handle* h) {
   CKLAUNCH("k_bhalf");
   TRY(nodes_and_field_energy<T, MIXED>(h, h->itime + 1));
   h->itime += 1;
+  return PBPIC_OK;
+}
+
+// The loop body of the reference (pic2d.f90:171-188): push, field solve and,
+// when due, the counting sort. The fused sort needs only the push's cell words
+// and tile counts and the field solve only the push's current, so after the
+// push the field solve runs on a second stream beside the sort and the handle's
+// stream waits for it before the next step: each step costs push + the longer
+// of the two. (The separate calls pbpic_push, pbpic_fieldsolve and pbpic_sort
+// stay in order on the handle's stream.)
+template <class T, bool MIXED>
+int do_step(pbpic_handle* h, int nsteps, int sort_every) {
+  const bool autosort = !(h->cfg.options & PBPIC_OPT_NO_AUTOSORT) && h->fused_ok;
+  for (int s = 0; s < nsteps; ++s) {
+    h->defer_sort = true;
+    const int rp = do_push<T, MIXED>(h);
+    h->defer_sort = false;
+    TRY(rp);
+    const bool due = autosort || (sort_every > 0 && (h->itime + 1) % sort_every == 0);
+    if (!(due && h->hist_valid)) {
+      TRY((do_fieldsolve<T, MIXED>(h)));
+      if (sort_every > 0 && h->itime % sort_every == 0) TRY((do_sort<T, MIXED>(h)));
+      continue;
+    }
+    if (!h->side) {
+      CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
+    CK(cudaEventRecord(h->ev_fork, h->stream));
+    CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    const cudaStream_t main = h->stream;
+    h->stream = h->side;
+    const int rf = do_fieldsolve<T, MIXED>(h);
+    h->stream = main;
+    const int rs = rf == PBPIC_OK ? do_fused_sort<T, MIXED>(h) : rf;
+    CK(cudaEventRecord(h->ev_join, h->side));  // joined on the error paths too
+    CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    TRY(rs);
+  }
   return PBPIC_OK;
 }
 
@@ -1020,6 +1063,12 @@ int pbpic_create(const pbpic_config* cfg, pbpic_handle** out) {
 int pbpic_destroy(pbpic_handle* h) {
   if (!h) return PBPIC_OK;
   cudaStreamSynchronize(h->stream);
+  if (h->side) {
+    cudaStreamSynchronize(h->side);
+    cudaStreamDestroy(h->side);
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   for (void* p : h->allocs) cudaFree(p);
   delete h;
   return PBPIC_OK;
@@ -1161,12 +1210,7 @@ int pbpic_sort(pbpic_handle* h) {
 int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every) {
   TRY(check_handle(h));
   if (nsteps < 0 || sort_every < 0) return fail(PBPIC_EINVAL, "nsteps and sort_every must be >= 0");
-  for (int s = 0; s < nsteps; ++s) {
-    TRY(pbpic_push(h));
-    TRY(pbpic_fieldsolve(h));
-    if (sort_every > 0 && h->itime % sort_every == 0) TRY(pbpic_sort(h));
-  }
-  return PBPIC_OK;
+  return DISPATCH(h, do_step, h, nsteps, sort_every);
 }
 
 int pbpic_energy_spectra(pbpic_handle* h, double de_electron, double de_ion, int32_t nbins, int64_t* counts) {
