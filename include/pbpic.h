@@ -189,7 +189,10 @@ int pbpic_fieldsolve(pbpic_handle* h);
 /* countingsort (pic2d.f90:1303-1329): stable sort of the particles by cell. */
 int pbpic_sort(pbpic_handle* h);
 /* The reference time loop body (pic2d.f90:171-188) nsteps times:
- * push, fieldsolve, and a sort every sort_every steps (0: never). */
+ * push, fieldsolve, and a sort every sort_every steps (0: never). When a
+ * step sorts, its field solve runs on a second stream of the library beside
+ * the sort and the handle's stream waits for it before the call returns
+ * control of the stream: the results equal the three calls in order. */
 int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every);
 /* Wait for the handle's stream. */
 int pbpic_synchronize(pbpic_handle* h);
