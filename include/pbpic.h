@@ -191,8 +191,8 @@ int pbpic_sort(pbpic_handle* h);
 /* The reference time loop body (pic2d.f90:171-188) nsteps times:
  * push, fieldsolve, and a sort every sort_every steps (0: never). When a
  * step sorts, its field solve runs on a second stream of the library beside
- * the sort and the handle's stream waits for it before the call returns
- * control of the stream: the results equal the three calls in order. */
+ * the sort, and the handle's stream waits for it (an event) before the next
+ * step: the results equal the three calls in order. */
 int pbpic_step(pbpic_handle* h, int32_t nsteps, int32_t sort_every);
 /* Wait for the handle's stream. */
 int pbpic_synchronize(pbpic_handle* h);
