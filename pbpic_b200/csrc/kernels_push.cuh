@@ -237,7 +237,9 @@ struct Pushed {
   uint32_t cw;           // new cell word
   T dx, dy, ux, uy, uz;  // new state (after reflection)
   int dcx, dcy, di, dj;  // cell steps and jz quadrant
-  T e[16];               // deposit terms: jx 4, jy 4, jz 4, rho 4
+  T e[16];               // deposit terms: jx 4, jy 4, jz 4, rho 4 (the exact order fills all 16; the
+                         // cell-relative form only the second segment's e[2], e[3], e[6], e[7] and
+                         // the stencil quantities below)
   // mixed form, cell-stencil form of the same deposit: jx at (0,0), (0,1) is
   // ja*(1-jw), ja*jw (first segment only for a crossing particle, the whole
   // move otherwise), jy at (0,0), (1,0) is jb*(1-jv), jb*jv; jz is quz times
@@ -329,12 +331,22 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
   const T sx = A::mul(t2, tx), sy = A::mul(t2, ty), sz = A::mul(t2, tz);
   const bool cb = COMPAT && (a.compat & 1) != 0;  // rotate the pre-kick momentum (pic2d.f90:985-987)
   const T vx = cb ? pux : umx, vy = cb ? puy : umy, vz0 = cb ? puz : umz;
-  const T u0x = A::add(umx, A::mad(vy, tz, -A::mul(vz0, ty)));
-  const T u0y = A::add(umy, A::mad(vz0, tx, -A::mul(vx, tz)));
-  const T u0z = A::add(umz, A::mad(vx, ty, -A::mul(vy, tx)));
-  const T upx = A::add(umx, A::mad(u0y, sz, -A::mul(u0z, sy)));
-  const T upy = A::add(umy, A::mad(u0z, sx, -A::mul(u0x, sz)));
-  const T upz = A::add(umz, A::mad(u0x, sy, -A::mul(u0y, sx)));
+  T u0x, u0y, u0z, upx, upy, upz;
+  if constexpr (MIXED || !COMPAT) {  // u' = u- + v x t and u+ = u- + u' x s as two fused multiply-adds a component
+    u0x = A::mad(vy, tz, A::mad(-vz0, ty, umx));
+    u0y = A::mad(vz0, tx, A::mad(-vx, tz, umy));
+    u0z = A::mad(vx, ty, A::mad(-vy, tx, umz));
+    upx = A::mad(u0y, sz, A::mad(-u0z, sy, umx));
+    upy = A::mad(u0z, sx, A::mad(-u0x, sz, umy));
+    upz = A::mad(u0x, sy, A::mad(-u0y, sx, umz));
+  } else {
+    u0x = A::add(umx, A::mad(vy, tz, -A::mul(vz0, ty)));
+    u0y = A::add(umy, A::mad(vz0, tx, -A::mul(vx, tz)));
+    u0z = A::add(umz, A::mad(vx, ty, -A::mul(vy, tx)));
+    upx = A::add(umx, A::mad(u0y, sz, -A::mul(u0z, sy)));
+    upy = A::add(umy, A::mad(u0z, sx, -A::mul(u0x, sz)));
+    upz = A::add(umz, A::mad(u0x, sy, -A::mul(u0y, sx)));
+  }
   const T ux = A::mad(c1, ex, upx), uy = A::mad(c1, ey, upy), uz = A::mad(c1, ez, upz);
   const T g2 = A::mad(uz, uz, A::mad(uy, uy, A::mad(ux, ux, one)));
   T c3, vz, gama;
@@ -401,12 +413,8 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
     const T fy1 = A::mul(qy, A::sub(jr, ys)), fy2 = A::mul(qy, A::sub(ye, jr));
     const T wx1 = A::mul(A::add(ir, xs), half), wy1 = A::mul(A::add(jr, ys), half);
     const T wx2 = A::sub(A::mul(A::add(ir, xe), half), fdcx), wy2 = A::sub(A::mul(A::add(jr, ye), half), fdcy);
-    o.e[0] = A::mad(-fx1, wy1, fx1);  // jx (0, 0)
-    o.e[1] = A::mul(fx1, wy1);        // jx (0, 1)
     o.e[2] = A::mad(-fx2, wy2, fx2);  // jx (dcx, dcy)
     o.e[3] = A::mul(fx2, wy2);        // jx (dcx, dcy+1)
-    o.e[4] = A::mad(-fy1, wx1, fy1);  // jy (0, 0)
-    o.e[5] = A::mul(fy1, wx1);        // jy (1, 0)
     o.e[6] = A::mad(-fy2, wx2, fy2);  // jy (dcx, dcy)
     o.e[7] = A::mul(fy2, wx2);        // jy (dcx+1, dcy)
     const bool cr = dcx != 0 || dcy != 0;
@@ -449,10 +457,12 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
     o.quz = quz;
     o.zdx = dimid;
     o.zdy = djmid;
-    o.e[8] = A::mul(quz, z4);   // jz (0, 0)
-    o.e[9] = A::mul(quz, z2);   // jz (di, 0)
-    o.e[10] = A::mul(quz, z3);  // jz (0, dj)
-    o.e[11] = A::mul(quz, z1);  // jz (di, dj)
+    if constexpr (!(MIXED || !COMPAT)) {
+      o.e[8] = A::mul(quz, z4);   // jz (0, 0)
+      o.e[9] = A::mul(quz, z2);   // jz (di, 0)
+      o.e[10] = A::mul(quz, z3);  // jz (0, dj)
+      o.e[11] = A::mul(quz, z1);  // jz (di, dj)
+    }
   }
   {
     const bool cr = COMPAT && (a.compat & 4) != 0;  // mirrored weights (pic2d.f90:1285-1288)
@@ -462,10 +472,12 @@ __device__ __forceinline__ void push_core(const PushParams<T>& a, int sp, int ix
     const T r2 = A::sub(rx, r1);
     const T r3 = A::sub(ry, r1);
     const T r4 = A::sub(A::sub(A::sub(one, r1), r2), r3);
-    o.e[12] = A::mul(r4, qq);  // rho (0, 0)
-    o.e[13] = A::mul(r2, qq);  // rho (1, 0)
-    o.e[14] = A::mul(r3, qq);  // rho (0, 1)
-    o.e[15] = A::mul(r1, qq);  // rho (1, 1)
+    if constexpr (!(MIXED || !COMPAT)) {
+      o.e[12] = A::mul(r4, qq);  // rho (0, 0)
+      o.e[13] = A::mul(r2, qq);  // rho (1, 0)
+      o.e[14] = A::mul(r3, qq);  // rho (0, 1)
+      o.e[15] = A::mul(r1, qq);  // rho (1, 1)
+    }
     o.q = qq;
     o.rw[0] = r4;
     o.rw[1] = r2;
@@ -1041,7 +1053,6 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           push_one<T, MIXED, COMPAT>(a, sp, ix, iy, px[0], py[0], pux[0], puy[0], puz[0], n00, n01, n10, n11, o);
         status |= o.status;
         const bool cross = o.dcx != 0 || o.dcy != 0;
-        if (HIST && cross && inwin) status |= hist_move<T, MIXED>(a, tw, wrd, &o.cw, o.dcx, ix, iy);
         if (inwin) {
           const int key = iy - y0;
           if (key != acc_key) {
@@ -1106,13 +1117,17 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
             using F = M<T, true>;
 #pragma unroll
             for (int k = 0; k < 4; ++k) acc[13 + k] = F::mad(o.q, o.rw[k], acc[13 + k]);
+          } else if constexpr (!COMPAT) {  // the products the exact order keeps in e[12..15]
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[13 + k] += M<T, true>::mul(o.rw[k], o.q);
           } else {
             acc[13] += o.e[12];
             acc[14] += o.e[13];
             acc[15] += o.e[14];
             acc[16] += o.e[15];
           }
-          if (cross) {  // second zig-zag segment, attached to the new cell
+          if (cross) {  // new-cell count and second zig-zag segment, in one branch
+            if (HIST) status |= hist_move<T, MIXED>(a, tw, wrd, &o.cw, o.dcx, ix, iy);
             const int wx = 1 + o.dcx, wy = key + 1 + o.dcy;
             const int b0 = (JX * 4 + wx) * WR + wy, b1 = (JY * 4 + wx) * WR + wy;
             if (split) {
@@ -1129,8 +1144,28 @@ __device__ __forceinline__ void push_tile(const PushParams<T>& a, const int t, P
           }
         } else {
           status |= 4;
+          if constexpr (MIXED || !COMPAT) {  // the 16 terms from the stencil quantities (rare path only)
+            using F = M<T, true>;
+            const T z = T(0);
+            mycol[0 * 33] = F::mad(-o.ja, o.jw, o.ja);
+            mycol[1 * 33] = F::mul(o.ja, o.jw);
+            mycol[2 * 33] = cross ? o.e[2] : z;
+            mycol[3 * 33] = cross ? o.e[3] : z;
+            mycol[4 * 33] = F::mad(-o.jb, o.jv, o.jb);
+            mycol[5 * 33] = F::mul(o.jb, o.jv);
+            mycol[6 * 33] = cross ? o.e[6] : z;
+            mycol[7 * 33] = cross ? o.e[7] : z;
+            const T qs = F::mul(o.quz, o.zdx), q0 = F::sub(o.quz, qs), y0 = F::sub(T(1), o.zdy);
+            mycol[8 * 33] = F::mul(q0, y0);
+            mycol[9 * 33] = F::mul(qs, y0);
+            mycol[10 * 33] = F::mul(q0, o.zdy);
+            mycol[11 * 33] = F::mul(qs, o.zdy);
 #pragma unroll
-          for (int k = 0; k < 16; ++k) mycol[k * 33] = o.e[k];
+            for (int k = 0; k < 4; ++k) mycol[(12 + k) * 33] = F::mul(o.q, o.rw[k]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) mycol[k * 33] = o.e[k];
+          }
           deposit_global<T, MIXED>(a.jacc, a.mx, a.my, a.S, a.ybc, a.compat, mycol, ix, iy, o.dcx, o.dcy, o.di, o.dj);
         }
         rot4(cw, o.cw);
