@@ -331,6 +331,17 @@ struct FusedSortParams {
   int32_t* base;           // [ntiles][nb] first slot of each (tile, bin)
 };
 
+// A cell whose 3x3 neighbours need no wrap or wall: the tiles whose windows hold it are the
+// tile rows (cy-1)/ty .. (cy+1)/ty of columns cx-1, cx, cx+1, and its bin in the tile of column
+// cx+dx and tile row tr is (1-dx, cy - tr*ty + 1) -- the same tiles and bins tiles_of_cell and
+// bin_in_tile find, in tile order (column, then row).
+__device__ __forceinline__ bool interior_cell(int cx, int cy, int mx, int my) {
+  return cx >= 1 && cx <= mx - 2 && cy >= 1 && cy <= my - 2;
+}
+__device__ __forceinline__ int64_t interior_bin_index(const FusedSortParams& a, int cx, int cy, int dx, int tr) {
+  return ((int64_t)(cx + dx) * a.tpc + tr) * a.nb + (1 - dx) * (a.ty + 2) + (cy - tr * a.ty + 1);
+}
+
 __device__ __forceinline__ void fused_counts_body(const FusedSortParams& a) {
   const int64_t ncells = (int64_t)a.mx * a.my;
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
@@ -339,12 +350,18 @@ __device__ __forceinline__ void fused_counts_body(const FusedSortParams& a) {
       continue;
     }
     const int cx = (int)(c / a.my), cy = (int)(c - (int64_t)cx * a.my);
-    int tl[9];
-    const int n = tiles_of_cell(cx, cy, a.mx, a.my, a.ybc, a.ty, a.tpc, tl);
     int32_t s = 0;
-    for (int k = 0; k < n; ++k) {
-      const int b = bin_in_tile(cx, cy, tl[k], a.mx, a.my, a.ybc, a.ty, a.tpc);
-      if (b >= 0) s += a.tilecnt[(int64_t)tl[k] * a.nb + b];
+    if (interior_cell(cx, cy, a.mx, a.my)) {
+      const int tlo = (cy - 1) / a.ty, thi = (cy + 1) / a.ty;
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int tr = tlo; tr <= thi; ++tr) s += a.tilecnt[interior_bin_index(a, cx, cy, dx, tr)];
+    } else {
+      int tl[9];
+      const int n = tiles_of_cell(cx, cy, a.mx, a.my, a.ybc, a.ty, a.tpc, tl);
+      for (int k = 0; k < n; ++k) {
+        const int b = bin_in_tile(cx, cy, tl[k], a.mx, a.my, a.ybc, a.ty, a.tpc);
+        if (b >= 0) s += a.tilecnt[(int64_t)tl[k] * a.nb + b];
+      }
     }
     a.counts[c] = s;
   }
@@ -389,6 +406,17 @@ static __global__ void k_fused_offsets(FusedSortParams a, const int32_t* sums) {
     a.off[c] = o;
     if (c == ncells) continue;
     const int cx = (int)(c / a.my), cy = (int)(c - (int64_t)cx * a.my);
+    if (interior_cell(cx, cy, a.mx, a.my)) {  // the (tile, bin) entries in tile order: a running sum
+      const int tlo = (cy - 1) / a.ty, thi = (cy + 1) / a.ty;
+      int32_t before = o;
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int tr = tlo; tr <= thi; ++tr) {
+          const int64_t e = interior_bin_index(a, cx, cy, dx, tr);
+          a.base[e] = before;
+          before += a.tilecnt[e];
+        }
+      continue;
+    }
     int tl[9], bl[9], cl[9];
     const int nt = tiles_of_cell(cx, cy, a.mx, a.my, a.ybc, a.ty, a.tpc, tl);
     for (int k = 0; k < nt; ++k) {
@@ -456,6 +484,9 @@ __device__ __forceinline__ void perm_tile(const ScatterParams<T>& a, const int t
   const int pbeg = a.tile_off[t], pend = a.tile_off[t + 1];
   const int w = threadIdx.x >> 5;
   const unsigned lane = lane_id(), lt = lanemask_lt();
+  // the window wraps only for the first and last columns and, with periodic y, the first and last tile rows
+  const bool edge = ixt == 0 || ixt == a.mx - 1 || (a.ybc == 0 && (y0 == 0 || y1 == a.my));
+  const int nrow = y1 - y0 + 1;  // window rows 0..nrow
   for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
     sm.run[b] = 0;
     sm.sbase[b] = a.base[(int64_t)t * a.nb + b];
@@ -465,26 +496,41 @@ __device__ __forceinline__ void perm_tile(const ScatterParams<T>& a, const int t
     __syncthreads();
     int bin[SP_IPT], pos[SP_IPT];
     uint32_t vc[SP_IPT];
+    if (c0 + SP_CHUNK <= pend && !edge) {
+      // a whole chunk of a tile whose window does not wrap: each bin straight from the cell steps
 #pragma unroll
-    for (int k = 0; k < SP_IPT; ++k) {  // every load of the chunk before the ranking
-      const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
-      vc[k] = p < pend ? a.ci[p] : 0u;
+      for (int k = 0; k < SP_IPT; ++k) vc[k] = a.ci[c0 + w * (32 * SP_IPT) + k * 32 + (int)lane];
+#pragma unroll
+      for (int k = 0; k < SP_IPT; ++k) {
+        const int bx = (int)cw_ix(vc[k]) - ixt + 1, by = (int)cw_iy(vc[k]) - y0 + 1;
+        bin[k] = ((unsigned)bx <= 2u && (unsigned)by <= (unsigned)nrow) ? bx * (a.ty + 2) + by : a.nb;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < SP_IPT; ++k) {  // every load of the chunk before the ranking
+        const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
+        vc[k] = p < pend ? a.ci[p] : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < SP_IPT; ++k) {
+        const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
+        int b = a.nb;  // sentinel: beyond the tile
+        if (p < pend) {
+          b = window_bin(cw_ix(vc[k]), cw_iy(vc[k]), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
+          if (b < 0) b = a.nb;  // cannot happen: the push kept every particle in its window
+        }
+        bin[k] = b;
+      }
     }
 #pragma unroll
     for (int k = 0; k < SP_IPT; ++k) {
-      const int p = c0 + w * (32 * SP_IPT) + k * 32 + (int)lane;
-      int b = a.nb;  // sentinel: beyond the tile
-      if (p < pend) {
-        b = window_bin(cw_ix(vc[k]), cw_iy(vc[k]), ixt, y0, y1, a.ty, a.mx, a.my, a.ybc);
-        if (b < 0) b = a.nb;  // cannot happen: the push kept every particle in its window
-      }
+      const int b = bin[k];
       const unsigned peers = __match_any_sync(FULL, b);
       const int before = cnt[w][b];
       __syncwarp();
       if ((peers & lt) == 0) cnt[w][b] = before + __popc(peers);
       __syncwarp();
       pos[k] = before + __popc(peers & lt);
-      bin[k] = b;
     }
     __syncthreads();
     for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
