@@ -61,20 +61,23 @@ __global__ void k_aos_in(const RefRec<R>* in, int64_t n, int mx, int my, uint32_
   }
 }
 
+// Record i is array element perm[i] (the sort's permutation, not yet applied to
+// the arrays) or element i (perm null).
 template <class T, class R>
-__global__ void k_aos_out(RefRec<R>* out, int64_t n, int my, const uint32_t* cell, const T* dx,
+__global__ void k_aos_out(RefRec<R>* out, int64_t n, int my, const int32_t* perm, const uint32_t* cell, const T* dx,
                           const T* dy, const T* ux, const T* uy, const T* uz, const int32_t* pid) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t w = cell[i];
+    const int64_t e = perm ? (int64_t)perm[i] : i;
+    const uint32_t w = cell[e];
     RefRec<R> r;
-    r.dx = (R)dx[i];
-    r.dy = (R)dy[i];
-    r.ux = (R)ux[i];
-    r.uy = (R)uy[i];
-    r.uz = (R)uz[i];
+    r.dx = (R)dx[e];
+    r.dy = (R)dy[e];
+    r.ux = (R)ux[e];
+    r.uy = (R)uy[e];
+    r.uz = (R)uz[e];
     r.grid = my * cw_ix(w) + cw_iy(w) + 1;
     r.q = cw_sp(w) ? -1 : 1;
-    r.pid = pid ? pid[i] : 0;
+    r.pid = pid ? pid[e] : 0;
     if constexpr (sizeof(RefRec<R>) == 56) r.pad = 0;
     out[i] = r;
   }

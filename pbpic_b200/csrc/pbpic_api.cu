@@ -797,13 +797,14 @@ int do_load_aos(pbpic_handle* h, const RefRec<R>* host, int64_t n) {
 
 template <class T, bool MIXED, class R>
 int do_store_aos(pbpic_handle* h, RefRec<R>* host, int64_t cap, int64_t* nout) {
-  TRY(materialize(h));
+  // a pending permutation is read through, not applied: the records come out in cell order either way
   if (nout) *nout = h->n;
   const int64_t n = std::min<int64_t>(cap, h->n);
   if (n <= 0) return PBPIC_OK;
   const int b = h->cur;
   TRY(ensure_staging(h, (size_t)n * sizeof(RefRec<R>)));
-  k_aos_out<T, R><<<grid_for(n, 256), 256, 0, h->stream>>>((RefRec<R>*)h->staging, n, h->cfg.my, h->cell[b],
+  k_aos_out<T, R><<<grid_for(n, 256), 256, 0, h->stream>>>((RefRec<R>*)h->staging, n, h->cfg.my,
+                                                             h->lazy ? h->perm : nullptr, h->cell[b],
                                                              P<T>(h, b, 0), P<T>(h, b, 1), P<T>(h, b, 2),
                                                              P<T>(h, b, 3), P<T>(h, b, 4), h->pid[b]);
   CKLAUNCH("k_aos_out");
